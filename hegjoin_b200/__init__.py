@@ -1,0 +1,345 @@
+"""hegjoin_b200 -- B200-native epsilon self-join (HEGJoin algorithm 0 drop-in).
+
+Python mirror of the reference's GPU-only join interface over the C ABI in
+``include/hegjoin_b200.h`` (libhegjoin_b200.so).  The reference's C++ entry
+points map one to one:
+
+    generateNDGridDimensions   (main.cu:449-520)      -> grid_geometry
+    gridIndexingGPU            (GPU.cu:74-398)        -> gridIndexingGPU / GridIndex
+    sortByWorkLoad             (SortByWorkload.cu:19) -> sortByWorkLoad / GridIndex.sort_by_workload
+    distanceTableNDGridBatches (GPU.cu:787-1702)      -> distanceTableNDGridBatches / join
+
+Device buffers are torch CUDA tensors; torch supplies memory and streams only.
+All compute runs in the CUDA library; there is no CPU fallback: if the shared
+library is missing, importing this package raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhegjoin_b200.so")
+
+HJ_OK = 0
+HJ_ERR_INVALID = 1
+HJ_ERR_CUDA = 2
+HJ_ERR_OOM = 3
+HJ_ERR_OVERFLOW = 4
+HJ_ERR_TIMEOUT = 5
+HJ_ERR_UNSUPPORTED = 6
+HJ_ERR_NO_DEVICE = 7
+HJ_F32 = 0
+HJ_F64 = 1
+HJ_REFINE_AUTO = 0
+HJ_REFINE_EXACT = 1
+HJ_REFINE_TC_F16 = 2
+HJ_REFINE_TC_BF16 = 3
+REFINE_NAMES = {"auto": 0, "exact": 1, "tc_f16": 2, "tc_bf16": 3}
+
+
+class HJError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"hegjoin_b200 status {status}: {msg}")
+        self.status = status
+
+
+class IndexInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("d", ctypes.c_uint32), ("k", ctypes.c_uint32), ("dtype", ctypes.c_uint32),
+                ("n_nonempty_cells", ctypes.c_uint32), ("grid_aliasing", ctypes.c_uint32),
+                ("total_cells", ctypes.c_uint64), ("total_candidates", ctypes.c_uint64),
+                ("eps", ctypes.c_double), ("sq_threshold", ctypes.c_double),
+                ("min_arr", ctypes.c_double * 16), ("n_cells", ctypes.c_uint32 * 16)]
+
+
+class JoinOpts(ctypes.Structure):
+    _fields_ = [("refine", ctypes.c_int), ("result_capacity", ctypes.c_uint64), ("sample_rate", ctypes.c_double),
+                ("mem_fraction", ctypes.c_double), ("query_block", ctypes.c_uint32), ("max_batches", ctypes.c_uint32),
+                ("use_graphs", ctypes.c_uint32), ("keep_keys", ctypes.c_uint32)]
+
+
+class JoinStats(ctypes.Structure):
+    _fields_ = [("total_pairs", ctypes.c_uint64), ("n_batches", ctypes.c_uint32), ("n_retries", ctypes.c_uint32),
+                ("band_pairs", ctypes.c_uint64), ("tc_accepts", ctypes.c_uint64), ("estimated_pairs", ctypes.c_uint64),
+                ("filter_delta", ctypes.c_double), ("ms_estimate", ctypes.c_float), ("ms_refine", ctypes.c_float),
+                ("ms_group", ctypes.c_float), ("ms_total", ctypes.c_float), ("refine_used", ctypes.c_uint32),
+                ("kernel_launches", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C hegjoin_b200/csrc` "
+                          "(or __graft_entry__.build()); there is no CPU fallback")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, U32, U64, I, D = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_double
+    sigs = {
+        "hj_last_error": (ctypes.c_char_p, []),
+        "hj_version": (ctypes.c_char_p, []),
+        "hj_kernel_launch_count": (U64, []),
+        "hj_grid_geometry": (I, [P, U32, U32, U32, I, D, P, P, P, P, P]),
+        "hj_index_create": (I, [P, U32, U32, U32, I, D, P, P, P, P]),
+        "hj_index_destroy": (I, [P]),
+        "hj_index_get_info": (I, [P, P]),
+        "hj_index_export": (I, [P, P, P, P, P]),
+        "hj_index_views": (I, [P, P, P, P, P]),
+        "hj_sort_by_workload": (I, [P, P, P]),
+        "hj_workload_export": (I, [P, P, P, P]),
+        "hj_join_opts_default": (None, [P]),
+        "hj_join": (I, [P, P, P, P, P]),
+        "hj_result_destroy": (I, [P]),
+        "hj_result_num_batches": (I, [P, P, P]),
+        "hj_result_batch": (I, [P, U32, P, P, P]),
+        "hj_result_table": (I, [P, P]),
+        "hj_result_to_csr": (I, [P, P, P, I, P]),
+        "hj_result_digest": (I, [P, P, P, P, P]),
+        "hj_self_join_host": (I, [P, U32, U32, U32, I, D, P, P, P, P]),
+        "hj_probe_sqdist": (I, [P, P, U32, U32, I, P, P]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    return (lib.hj_last_error() or b"").decode()
+
+
+def check(status: int) -> None:
+    if status != HJ_OK:
+        raise HJError(status, last_error())
+
+
+def kernel_launch_count() -> int:
+    return int(lib.hj_kernel_launch_count())
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream) -> int | None:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream or None
+
+
+def _dtype_code(t) -> int:
+    torch = _torch()
+    if t.dtype == torch.float32:
+        return HJ_F32
+    if t.dtype == torch.float64:
+        return HJ_F64
+    raise ValueError(f"unsupported dataset dtype {t.dtype} (float32 or float64)")
+
+
+def _ptr(t) -> int:
+    return t.data_ptr()
+
+
+def grid_geometry(db, k: int, eps: float, stream=None):
+    """generateNDGridDimensions (main.cu:449-520): (minArr, maxArr, nCells, totalCells)."""
+    n, d = db.shape
+    mn = (ctypes.c_double * k)()
+    mx = (ctypes.c_double * k)()
+    nc = (ctypes.c_uint32 * k)()
+    tot = ctypes.c_uint64()
+    check(lib.hj_grid_geometry(_ptr(db), n, d, k, _dtype_code(db), float(eps), mn, mx, nc, ctypes.byref(tot),
+                               _stream_ptr(stream)))
+    return list(mn), list(mx), list(nc), int(tot.value)
+
+
+class GridIndex:
+    """Device grid index over an n x d dataset (gridIndexingGPU, GPU.cu:74-398)."""
+
+    def __init__(self, db, k: int, eps: float, min_arr=None, n_cells=None, stream=None):
+        torch = _torch()
+        if not db.is_cuda or not db.is_contiguous():
+            raise ValueError("db must be a contiguous CUDA tensor")
+        self.db = db
+        n, d = db.shape
+        self._stream = stream
+        h = ctypes.c_void_p()
+        mn = (ctypes.c_double * k)(*min_arr) if min_arr is not None else None
+        nc = (ctypes.c_uint32 * k)(*n_cells) if n_cells is not None else None
+        check(lib.hj_index_create(_ptr(db), n, d, k, _dtype_code(db), float(eps), mn, nc, _stream_ptr(stream),
+                                  ctypes.byref(h)))
+        self._h = h
+        self.torch = torch
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.hj_index_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> IndexInfo:
+        inf = IndexInfo()
+        check(lib.hj_index_get_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    def export(self):
+        """(gridCellLookup linear ids, grid indexmin, grid indexmax, indexLookupArr) as CUDA tensors."""
+        torch = self.torch
+        inf = self.info()
+        nc, n = inf.n_nonempty_cells, inf.n
+        lookup = torch.empty((max(nc, 1), 2), dtype=torch.int64, device=self.db.device)
+        grid = torch.empty((max(nc, 1), 2), dtype=torch.int32, device=self.db.device)
+        ilu = torch.empty(n, dtype=torch.int32, device=self.db.device)
+        check(lib.hj_index_export(self._h, _ptr(lookup), _ptr(grid), _ptr(ilu), _stream_ptr(self._stream)))
+        idx = (lookup[:nc, 0] & 0xFFFFFFFF)
+        return lookup[:nc, 1], grid[:nc, 0], grid[:nc, 1], ilu, idx
+
+    def views(self):
+        pts = ctypes.c_void_p(); perm = ctypes.c_void_p(); lid = ctypes.c_void_p(); cs = ctypes.c_void_p()
+        check(lib.hj_index_views(self._h, ctypes.byref(pts), ctypes.byref(perm), ctypes.byref(lid), ctypes.byref(cs)))
+        return pts.value, perm.value, lid.value, cs.value
+
+    def sort_by_workload(self) -> int:
+        tot = ctypes.c_uint64()
+        check(lib.hj_sort_by_workload(self._h, _stream_ptr(self._stream), ctypes.byref(tot)))
+        return int(tot.value)
+
+    def workload_export(self):
+        """(schedulingCell[nNonEmpty] as (nbPoints, cellId) int32 pairs, originPointIndex[n])."""
+        torch = self.torch
+        inf = self.info()
+        sched = torch.empty((max(inf.n_nonempty_cells, 1), 2), dtype=torch.int32, device=self.db.device)
+        origin = torch.empty(inf.n, dtype=torch.int32, device=self.db.device)
+        check(lib.hj_workload_export(self._h, _ptr(sched), _ptr(origin), _stream_ptr(self._stream)))
+        return sched[:inf.n_nonempty_cells], origin
+
+
+class JoinResult:
+    """Device result of a join: per-batch neighbour ids grouped by query, plus the neighbour table."""
+
+    def __init__(self, handle, stats: JoinStats, n: int, device):
+        self._h = handle
+        self.stats = stats
+        self.n = n
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.hj_result_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def total_pairs(self) -> int:
+        return int(self.stats.total_pairs)
+
+    def to_csr(self, sort_lists: bool = True, stream=None):
+        torch = _torch()
+        off = torch.empty(self.n + 1, dtype=torch.int64, device=self.device)
+        vals = torch.empty(max(self.total_pairs, 1), dtype=torch.int32, device=self.device)
+        check(lib.hj_result_to_csr(self._h, _ptr(off), _ptr(vals), int(sort_lists), _stream_ptr(stream)))
+        return off, vals[:self.total_pairs]
+
+    def digest(self, stream=None):
+        torch = _torch()
+        cnt = torch.empty(self.n, dtype=torch.int32, device=self.device)
+        s = torch.empty(self.n, dtype=torch.int64, device=self.device)
+        x = torch.empty(self.n, dtype=torch.int64, device=self.device)
+        check(lib.hj_result_digest(self._h, _ptr(cnt), _ptr(s), _ptr(x), _stream_ptr(stream)))
+        return cnt, s, x
+
+    def batches(self):
+        nb = ctypes.c_uint32(); tot = ctypes.c_uint64()
+        check(lib.hj_result_num_batches(self._h, ctypes.byref(nb), ctypes.byref(tot)))
+        out = []
+        for b in range(nb.value):
+            v = ctypes.c_void_p(); k = ctypes.c_void_p(); c = ctypes.c_uint64()
+            check(lib.hj_result_batch(self._h, b, ctypes.byref(v), ctypes.byref(k), ctypes.byref(c)))
+            out.append((v.value, k.value, int(c.value)))
+        return out
+
+    def table_ptr(self) -> int:
+        t = ctypes.c_void_p()
+        check(lib.hj_result_table(self._h, ctypes.byref(t)))
+        return t.value
+
+
+def join_opts(refine="auto", result_capacity=0, sample_rate=0.0, mem_fraction=0.0, max_batches=0,
+              use_graphs=False, keep_keys=False) -> JoinOpts:
+    o = JoinOpts()
+    lib.hj_join_opts_default(ctypes.byref(o))
+    o.refine = REFINE_NAMES[refine] if isinstance(refine, str) else int(refine)
+    o.result_capacity = int(result_capacity)
+    if sample_rate:
+        o.sample_rate = float(sample_rate)
+    if mem_fraction:
+        o.mem_fraction = float(mem_fraction)
+    o.max_batches = int(max_batches)
+    o.use_graphs = int(bool(use_graphs))
+    o.keep_keys = int(bool(keep_keys))
+    return o
+
+
+def join(index: GridIndex, stream=None, **kw) -> JoinResult:
+    """distanceTableNDGridBatches (GPU.cu:787-1702) for algorithm 0, result kept on the device."""
+    o = join_opts(**kw)
+    st = JoinStats()
+    h = ctypes.c_void_p()
+    check(lib.hj_join(index.handle, ctypes.byref(o), _stream_ptr(stream), ctypes.byref(h), ctypes.byref(st)))
+    return JoinResult(h, st, index.info().n, index.db.device)
+
+
+def self_join_host(db: np.ndarray, k: int, eps: float, stream=None, keep=True, **kw):
+    """One-shot join from host memory (copies in, index, workload order, join)."""
+    db = np.ascontiguousarray(db)
+    dt = HJ_F32 if db.dtype == np.float32 else HJ_F64
+    o = join_opts(**kw)
+    st = JoinStats()
+    h = ctypes.c_void_p()
+    check(lib.hj_self_join_host(db.ctypes.data, db.shape[0], db.shape[1], k, dt, float(eps), ctypes.byref(o),
+                                _stream_ptr(stream), ctypes.byref(h) if keep else None, ctypes.byref(st)))
+    torch = _torch()
+    return JoinResult(h if keep else ctypes.c_void_p(), st, db.shape[0], torch.device("cuda"))
+
+
+# ---- names of the reference's entry points ---------------------------------------------
+def gridIndexingGPU(db, k: int, eps: float, min_arr=None, n_cells=None, stream=None) -> GridIndex:
+    return GridIndex(db, k, eps, min_arr, n_cells, stream)
+
+
+def sortByWorkLoad(index: GridIndex) -> int:
+    return index.sort_by_workload()
+
+
+def distanceTableNDGridBatches(index: GridIndex, **kw) -> JoinResult:
+    return join(index, **kw)
+
+
+def probe_sqdist(a, b, stream=None):
+    """Evaluate kernel.cu:350-353's expression as nvcc compiles it by default (row-wise pairs)."""
+    torch = _torch()
+    n, d = a.shape
+    out = torch.empty(n, dtype=a.dtype, device=a.device)
+    check(lib.hj_probe_sqdist(_ptr(a), _ptr(b), n, d, _dtype_code(a), _ptr(out), _stream_ptr(stream)))
+    return out

@@ -1,0 +1,301 @@
+// hj_refine_plain.cu -- exact refine on the CUDA cores.
+//
+// Reference counterpart: kernelNDGridIndexGlobal (kernel.cu:727-802) with
+// evaluateCell (kernel.cu:378-412) and evalPoint (kernel.cu:333-370), and the
+// estimator kernel kernelNDGridIndexBatchEstimator_v2 (kernel.cu:607-716),
+// which is this kernel in count-only mode.
+//
+// Semantics kept bit for bit: a pair (q, c) is emitted iff c lies in one of
+// the non-empty cells of q's 3^k stencil (unsigned clamp with the wrap at
+// coordinate 0, kernel.cu:780-781) and
+//     acc = 0; for l in 0..d-1: diff = c_l - q_l; acc = fma(diff, diff, acc)
+// satisfies sqrt(acc) <= eps, evaluated as acc <= thr where thr is the largest
+// value of the dataset type whose correctly rounded sqrt is <= eps.
+//
+// B200 design: a persistent grid pulls work items (up to QB queries of one
+// cell) from the workload-ordered block list with one atomic per item.  The
+// cell's stencil is resolved once per item into contiguous point ranges
+// (rows of the stencil along dimension 0), the candidates are streamed through
+// shared memory in chunks of CB points (transposed to dimension-major), and
+// each thread evaluates an RQ x RC register tile of (query, candidate) pairs.
+// Hits are appended with warp-aggregated reservations into the pair sink.
+
+#include "hj_internal.h"
+
+namespace hj {
+namespace {
+
+constexpr uint32_t kRowGroup = 256;   // stencil rows resolved per pass
+constexpr uint32_t kNoPos = 0xFFFFFFFFu;
+
+template <typename T>
+struct PlainArgs {
+    const T* pts;
+    const uint32_t* perm;
+    const unsigned long long* cell_lid;
+    const uint32_t* cell_start;
+    uint32_t nC;
+    uint32_t d;
+    HjGrid grid;
+    T thr;
+    const HjBlock* blocks;
+    uint32_t nblocks;
+    unsigned int* head;
+    PairSink sink;
+    uint32_t count_only;
+    unsigned long long* block_counts;   // count-only mode: pairs per work item
+};
+
+__device__ __forceinline__ uint32_t lower_bound_lid(const unsigned long long* a, uint32_t n, unsigned long long v) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double ffma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+template <typename T, int D, int QB, int CB, int RQ, int RC>
+__global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
+    static_assert((QB / RQ) * (CB / RC) == 256, "tile must map onto 256 threads");
+    static_assert(RQ * RC <= 32, "hit mask is 32 bits");
+    constexpr int TX = CB / RC;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t d = D ? (uint32_t)D : a.d;
+    T* q_s = reinterpret_cast<T*>(smem);                        // [d][QB]
+    T* c_s = q_s + (size_t)d * QB;                              // [d][CB]
+    uint32_t* qid_s = reinterpret_cast<uint32_t*>(c_s + (size_t)d * CB);  // [QB]
+    uint32_t* cpos_s = qid_s + QB;                              // [CB]
+    uint32_t* rs = cpos_s + CB;                                 // [kRowGroup] range starts
+    uint32_t* rp = rs + kRowGroup;                              // [kRowGroup + 1] prefix of lengths
+    __shared__ uint32_t s_item;
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t tx = tid % TX, ty = tid / TX;
+    const uint32_t k = a.grid.k;
+    WarpChunk wc;
+    warp_chunk_init(wc);
+
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(a.head, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= a.nblocks) break;
+        const HjBlock blk = a.blocks[item];
+        const uint32_t nq = blk.q1 - blk.q0;
+
+        // queries, dimension-major
+        for (uint32_t f = tid; f < (uint32_t)QB * d; f += 256) {
+            uint32_t i = f / d, l = f - i * d;
+            q_s[l * QB + i] = i < nq ? a.pts[(size_t)(blk.q0 + i) * d + l] : T(0);
+        }
+        for (uint32_t i = tid; i < (uint32_t)QB; i += 256) qid_s[i] = i < nq ? a.perm[blk.q0 + i] : 0u;
+
+        // stencil box from the cell's linear id (its digits are every member's coordinates)
+        const unsigned long long L = a.cell_lid[blk.cell];
+        uint32_t lo[kMaxK], w[kMaxK];
+        uint32_t rows = 1;
+        bool empty = false;
+        for (uint32_t j = 0; j < k; ++j) {
+            uint32_t c = (j + 1 < k) ? (uint32_t)((L / a.grid.mult[j]) % a.grid.n_cells[j])
+                                     : (uint32_t)(L / a.grid.mult[j]);
+            uint32_t l = c - 1u;                                // kernel.cu:780, wraps at 0
+            uint32_t h = min(a.grid.n_cells[j] - 1u, c + 1u);   // kernel.cu:781
+            empty |= l > h;
+            lo[j] = l;
+            w[j] = h - l + 1u;
+            if (j > 0) rows *= w[j];
+        }
+        unsigned long long item_cnt = 0;
+        if (!empty) {
+            for (uint32_t row0 = 0; row0 < rows; row0 += kRowGroup) {
+                const uint32_t nr = min(kRowGroup, rows - row0);
+                __syncthreads();
+                if (tid < 32) {
+                    // resolve the rows of this group into point ranges, then prefix their lengths
+                    uint32_t lens[kRowGroup / 32];
+                    uint32_t my = 0;
+#pragma unroll
+                    for (uint32_t s = 0; s < kRowGroup / 32; ++s) {
+                        uint32_t r = tid * (kRowGroup / 32) + s;
+                        uint32_t len = 0, st = 0;
+                        if (r < nr) {
+                            uint32_t rem = row0 + r;
+                            unsigned long long base = 0;
+                            for (uint32_t j = 1; j < k; ++j) {
+                                uint32_t t = lo[j] + rem % w[j];
+                                rem /= w[j];
+                                base += (unsigned long long)t * a.grid.mult[j];
+                            }
+                            unsigned long long la = base + lo[0], lb = la + w[0] - 1;
+                            uint32_t c0 = lower_bound_lid(a.cell_lid, a.nC, la), c1 = c0;
+                            while (c1 < a.nC && a.cell_lid[c1] <= lb) ++c1;
+                            st = a.cell_start[c0];
+                            len = a.cell_start[c1] - st;
+                            rs[r] = st;
+                        }
+                        lens[s] = len;
+                        my += len;
+                    }
+                    uint32_t incl = my;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (tid >= (uint32_t)o) incl += t;
+                    }
+                    uint32_t run = incl - my;
+#pragma unroll
+                    for (uint32_t s = 0; s < kRowGroup / 32; ++s) {
+                        uint32_t r = tid * (kRowGroup / 32) + s;
+                        if (r < nr) rp[r] = run;
+                        run += lens[s];
+                    }
+                    if (tid == 31) rp[nr] = incl;
+                }
+                __syncthreads();
+                const uint32_t total = rp[nr];
+                for (uint32_t cb = 0; cb < total; cb += CB) {
+                    for (uint32_t j = tid; j < (uint32_t)CB; j += 256) {
+                        uint32_t v = cb + j, p = kNoPos;
+                        if (v < total) {
+                            uint32_t lo2 = 0, hi2 = nr;   // last r with rp[r] <= v
+                            while (hi2 - lo2 > 1) {
+                                uint32_t mid = (lo2 + hi2) >> 1;
+                                if (rp[mid] <= v) lo2 = mid; else hi2 = mid;
+                            }
+                            p = rs[lo2] + (v - rp[lo2]);
+                        }
+                        cpos_s[j] = p;
+                    }
+                    __syncthreads();
+                    for (uint32_t f = tid; f < (uint32_t)CB * d; f += 256) {
+                        uint32_t l = f / CB, j = f - l * CB;
+                        uint32_t p = cpos_s[j];
+                        c_s[f] = p != kNoPos ? a.pts[(size_t)p * d + l] : T(0);
+                    }
+                    __syncthreads();
+                    const uint32_t nvalid = min((uint32_t)CB, total - cb);
+
+                    T acc[RQ][RC];
+#pragma unroll
+                    for (int r = 0; r < RQ; ++r)
+#pragma unroll
+                        for (int c = 0; c < RC; ++c) acc[r][c] = T(0);
+#pragma unroll(D ? (D < 32 ? D : 8) : 1)
+                    for (uint32_t l = 0; l < d; ++l) {
+                        T qv[RQ], cv[RC];
+#pragma unroll
+                        for (int r = 0; r < RQ; ++r) qv[r] = q_s[l * QB + ty * RQ + r];
+#pragma unroll
+                        for (int c = 0; c < RC; ++c) cv[c] = c_s[l * CB + tx * RC + c];
+#pragma unroll
+                        for (int r = 0; r < RQ; ++r)
+#pragma unroll
+                            for (int c = 0; c < RC; ++c) {
+                                T diff = fsub(cv[c], qv[r]);          // candidate - query (kernel.cu:351)
+                                acc[r][c] = ffma(diff, diff, acc[r][c]);
+                            }
+                    }
+                    uint32_t mask = 0;
+#pragma unroll
+                    for (int r = 0; r < RQ; ++r)
+#pragma unroll
+                        for (int c = 0; c < RC; ++c) {
+                            bool hit = acc[r][c] <= a.thr && (ty * RQ + r) < nq && (tx * RC + c) < nvalid;
+                            mask |= (hit ? 1u : 0u) << (r * RC + c);
+                        }
+                    if (a.count_only) {
+                        item_cnt += __popc(mask);
+                    } else {
+                        uint32_t m = mask;
+                        warp_emit(a.sink, wc, __popc(mask), [&](uint32_t) {
+                            uint32_t b = __ffs(m) - 1;
+                            m &= m - 1;
+                            uint32_t qi = ty * RQ + b / RC, cj = tx * RC + b % RC;
+                            return make_uint2(qid_s[qi], a.perm[cpos_s[cj]]);
+                        });
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+        if (a.count_only) {
+            for (int o = 16; o > 0; o >>= 1) item_cnt += __shfl_down_sync(0xffffffffu, item_cnt, o);
+            if (lane_id() == 0 && item_cnt) atomicAdd(&a.block_counts[item], item_cnt);
+        }
+        __syncthreads();
+    }
+    if (!a.count_only) warp_chunk_close(a.sink, wc);
+}
+
+template <typename T, int D, int QB, int CB, int RQ, int RC>
+hj_status launch_t(const PlainArgs<T>& args, cudaStream_t st) {
+    size_t smem = (size_t)(D ? D : args.d) * (QB + CB) * sizeof(T) + (QB + CB + 2 * kRowGroup + 1) * sizeof(uint32_t);
+    auto kern = k_refine_plain<T, D, QB, CB, RQ, RC>;
+    static size_t configured = 0;
+    if (smem > 48 * 1024 && smem > configured) {
+        HJ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = smem;
+    }
+    int per_sm = 0;
+    HJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    if (per_sm < 1) {
+        set_error("refine: %zu bytes of shared memory per block do not fit", smem);
+        return HJ_ERR_UNSUPPORTED;
+    }
+    unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * num_sms(), std::max<uint32_t>(args.nblocks, 1));
+    kern<<<grid, 256, smem, st>>>(args);
+    HJ_LAUNCHED();
+    return HJ_OK;
+}
+
+template <typename T>
+hj_status dispatch_t(const PlainArgs<T>& args, cudaStream_t st);
+
+template <>
+hj_status dispatch_t<float>(const PlainArgs<float>& a, cudaStream_t st) {
+    switch (a.d) {
+        case 2: return launch_t<float, 2, 64, 128, 4, 8>(a, st);
+        case 3: return launch_t<float, 3, 64, 128, 4, 8>(a, st);
+        case 6: return launch_t<float, 6, 64, 128, 4, 8>(a, st);
+        case 18: return launch_t<float, 18, 64, 128, 4, 8>(a, st);
+        case 32: return launch_t<float, 32, 64, 128, 4, 8>(a, st);
+        case 90: return launch_t<float, 90, 64, 128, 4, 8>(a, st);
+        default: return launch_t<float, 0, 64, 128, 4, 8>(a, st);
+    }
+}
+template <>
+hj_status dispatch_t<double>(const PlainArgs<double>& a, cudaStream_t st) {
+    switch (a.d) {
+        case 2: return launch_t<double, 2, 64, 64, 4, 4>(a, st);
+        case 3: return launch_t<double, 3, 64, 64, 4, 4>(a, st);
+        case 6: return launch_t<double, 6, 64, 64, 4, 4>(a, st);
+        default: return launch_t<double, 0, 64, 64, 4, 4>(a, st);
+    }
+}
+
+}  // namespace
+
+uint32_t plain_query_block(int dtype) { return 64; (void)dtype; }
+
+// Runs the exact refine over work items blocks[0..nblocks).  `head` must be
+// zero on entry.  count_only: per-item pair counts go to block_counts.
+hj_status launch_refine_plain(const hj_index* ix, const HjBlock* blocks, uint32_t nblocks, unsigned int* head,
+                              const PairSink& sink, uint32_t count_only, unsigned long long* block_counts,
+                              cudaStream_t st) {
+    if (nblocks == 0) return HJ_OK;
+    if (ix->dtype == HJ_F32) {
+        PlainArgs<float> a{(const float*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, ix->d, ix->grid,
+                           (float)ix->thr, blocks, nblocks, head, sink, count_only, block_counts};
+        return dispatch_t<float>(a, st);
+    }
+    PlainArgs<double> a{(const double*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, ix->d, ix->grid,
+                        ix->thr, blocks, nblocks, head, sink, count_only, block_counts};
+    return dispatch_t<double>(a, st);
+}
+
+}  // namespace hj

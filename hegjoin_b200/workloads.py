@@ -1,0 +1,157 @@
+"""Seeded synthetic workloads for the epsilon self-join.
+
+The reference ships a generator (datasets/dataset_gen_fixed_len_expo_dist.cpp:24-91)
+that draws each coordinate i.i.d. from Exp(rate=40) with ``std::mt19937`` and
+redraws values above 1.  The workloads here keep that distribution but use a
+counter-based generator so any slice of a dataset can be produced in parallel
+and reproduced bit for bit on any machine with the same numpy build:
+
+    u(seed, i, a) = (mix64(mix64(seed ^ SALT) + 64*i + a) >> 11) * 2**-53   in [0, 1)
+    x = -log1p(-u) / 40        (float64), cast to the dataset dtype,
+    attempt a = 0, 1, ... until the cast value is < 1.
+
+``i`` is the flat coordinate index (point * d + dim).  The Gaussian-cluster part
+of the skewed workload uses Box-Muller on two further streams.
+
+Each workload names its shape (n, d, k, dtype), seed and epsilon; epsilon for
+the calibrated workloads is the value found by ``calibrate_eps`` on a seeded 1%
+query sample (stored to 17 significant digits in EPS_TABLE).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+SALT = 0xD1B54A32D192ED03
+M64 = (1 << 64) - 1
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    """splitmix64 finaliser on a uint64 array (wrapping arithmetic)."""
+    with np.errstate(over="ignore"):
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def _uniform(seed: int, stream: int, idx: np.ndarray, attempt: int) -> np.ndarray:
+    base = _mix64(np.array([(seed ^ SALT ^ (stream * 0x632BE59BD9B4E019)) & M64], dtype=np.uint64))[0]
+    with np.errstate(over="ignore"):
+        z = _mix64(base + idx.astype(np.uint64) * np.uint64(64) + np.uint64(attempt))
+    return (z >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+
+
+def exp40(seed: int, n: int, d: int, dtype=np.float32, stream: int = 0) -> np.ndarray:
+    """n x d coordinates, i.i.d. Exp(rate=40) redrawn into [0, 1) after the dtype cast."""
+    total = n * d
+    out = np.empty(total, dtype=dtype)
+    chunk = 1 << 22
+    for s in range(0, total, chunk):
+        idx = np.arange(s, min(total, s + chunk), dtype=np.uint64)
+        pending = np.arange(idx.size)
+        vals = np.empty(idx.size, dtype=dtype)
+        attempt = 0
+        while pending.size:
+            u = _uniform(seed, stream, idx[pending], attempt)
+            x = (-np.log1p(-u) / 40.0).astype(dtype)
+            ok = x < dtype(1.0)
+            vals[pending[ok]] = x[ok]
+            pending = pending[~ok]
+            attempt += 1
+            if attempt >= 64:
+                raise RuntimeError("exp40: redraw limit reached")
+        out[s:s + idx.size] = vals
+    return out.reshape(n, d)
+
+
+def skewed(seed: int, n: int, d: int, n_clusters: int = 64, sigma: float = 0.002,
+           frac_clustered: float = 0.2, dtype=np.float32) -> np.ndarray:
+    """80% Exp(40) points and 20% from Gaussian clusters, clipped to [0, 1)."""
+    n_c = int(round(n * frac_clustered))
+    n_e = n - n_c
+    x = np.empty((n, d), dtype=dtype)
+    x[:n_e] = exp40(seed, n_e, d, dtype, stream=0)
+    centres = _uniform(seed, 1, np.arange(n_clusters * d, dtype=np.uint64), 0).reshape(n_clusters, d)
+    cid = (_mix64(np.arange(n_c, dtype=np.uint64) + np.uint64(seed * 7919)) % np.uint64(n_clusters)).astype(np.int64)
+    idx = np.arange(n_c * d, dtype=np.uint64)
+    u1 = _uniform(seed, 2, idx, 0)
+    u2 = _uniform(seed, 3, idx, 0)
+    g = np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * math.pi * u2)
+    pts = centres[cid] + sigma * g.reshape(n_c, d)
+    pts = np.clip(pts, 0.0, np.nextafter(1.0, 0.0))
+    c = pts.astype(dtype)
+    c[c >= dtype(1.0)] = np.nextafter(dtype(1.0), dtype(0.0))
+    x[n_e:] = c
+    return x
+
+
+@dataclasses.dataclass(frozen=True)
+class Workload:
+    name: str
+    n: int
+    d: int
+    k: int
+    dtype: str          # "f32" or "f64"
+    seed: int
+    eps: float          # epsilon in the dataset dtype (exactly representable)
+    target_neighbours: float | None = None
+    kind: str = "exp40"
+
+    @property
+    def np_dtype(self):
+        return np.float32 if self.dtype == "f32" else np.float64
+
+    def generate(self, n: int | None = None) -> np.ndarray:
+        n = self.n if n is None else n
+        if self.kind == "skewed":
+            return skewed(self.seed, n, self.d, dtype=self.np_dtype)
+        return exp40(self.seed, n, self.d, self.np_dtype)
+
+
+# Epsilon values found by calibrate_eps (1% seeded query sample against the full
+# dataset, bisection to the target mean neighbour count), as dataset-dtype values.
+EPS_TABLE = {
+    "c2_18d": 0.038387289,
+    "c3_90d": 0.20277268,
+    "c4_skew6d": 0.0,   # filled in by calibration
+}
+
+WORKLOADS = {
+    "c1_2d": Workload("c1_2d", 2_000_000, 2, 2, "f64", 0, 0.002),
+    "c2_18d": Workload("c2_18d", 5_000_000, 18, 6, "f32", 1, EPS_TABLE["c2_18d"], 50.0),
+    "c3_90d": Workload("c3_90d", 500_000, 90, 6, "f32", 2, EPS_TABLE["c3_90d"], 30.0),
+    "c4_skew6d": Workload("c4_skew6d", 10_000_000, 6, 6, "f32", 3, EPS_TABLE["c4_skew6d"], 200.0, "skewed"),
+}
+
+
+def mean_neighbours_sample(x: np.ndarray, eps: float, sample_frac: float = 0.01, seed: int = 12345,
+                           device: str = "cuda") -> float:
+    """Mean plain Euclidean neighbour count (self included) of a seeded query sample."""
+    import torch
+    n = x.shape[0]
+    m = max(1, int(n * sample_frac))
+    rng = np.random.default_rng(seed)
+    qi = np.sort(rng.choice(n, size=m, replace=False))
+    X = torch.from_numpy(x).to(device=device, dtype=torch.float32)
+    Q = X[torch.from_numpy(qi).to(device)]
+    tot = 0
+    for s in range(0, m, 1024):
+        d2 = torch.cdist(Q[s:s + 1024], X).square_()
+        tot += int((d2 <= eps * eps).sum().item())
+    return tot / m
+
+
+def calibrate_eps(x: np.ndarray, target: float, sample_frac: float = 0.01, seed: int = 12345,
+                  device: str = "cuda", iters: int = 40) -> float:
+    """Bisect epsilon so the sampled mean neighbour count reaches `target`."""
+    lo, hi = 0.0, 1.0
+    for _ in range(iters):
+        mid = 0.5 * (lo + hi)
+        if mean_neighbours_sample(x, mid, sample_frac, seed, device) < target:
+            lo = mid
+        else:
+            hi = mid
+    return float(np.float32(hi))

@@ -1,0 +1,204 @@
+/* hegjoin_b200.h -- C ABI of the B200-native epsilon self-join.
+ *
+ * This is the drop-in boundary for HEGJoin's GPU-only join (algorithm 0,
+ * `./main dataset epsilon dim 0`).  Each entry point below replaces one
+ * reference routine; the citation names the reference interface it stands in
+ * for.  The reference-signature C++ shims (gridIndexingGPU, sortByWorkLoad,
+ * distanceTableNDGridBatches) in hegjoin_b200/compat/ are written on top of
+ * these calls.
+ *
+ * Conventions
+ *   - Every call returns an hj_status (0 = HJ_OK).  hj_last_error() returns a
+ *     message for the most recent failure on the calling thread.
+ *   - Pointers named d_* are device pointers; h_* are host pointers.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Calls enqueue work on it; only calls documented as synchronising wait.
+ *   - Floating-point arguments that hold a dataset value (epsilon, minArr) are
+ *     passed as double and converted to the dataset type (float for HJ_F32),
+ *     the way main.cu:56 converts argv's epsilon to DTYPE.
+ *   - Indices are 32-bit (the reference stores point ids as unsigned/int).
+ */
+#ifndef HEGJOIN_B200_H
+#define HEGJOIN_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int hj_status;
+#define HJ_OK 0
+#define HJ_ERR_INVALID 1      /* bad argument or unsupported shape */
+#define HJ_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define HJ_ERR_OOM 3          /* device allocation failed */
+#define HJ_ERR_OVERFLOW 4     /* a result buffer was too small (batch is retried internally) */
+#define HJ_ERR_TIMEOUT 5      /* a bounded device-side wait expired */
+#define HJ_ERR_UNSUPPORTED 6  /* input outside the supported domain (see message) */
+#define HJ_ERR_NO_DEVICE 7    /* no CUDA device / kernel image for this GPU */
+
+#define HJ_F32 0
+#define HJ_F64 1
+
+/* Refine kernels. */
+#define HJ_REFINE_AUTO 0      /* tensor-core filter for d >= 16 with float data, else exact */
+#define HJ_REFINE_EXACT 1     /* CUDA-core refine in the dataset type, reference order */
+#define HJ_REFINE_TC_F16 2    /* tcgen05 FP16-input / FP32-accumulate filter + exact recheck */
+#define HJ_REFINE_TC_BF16 3   /* tcgen05 BF16-input / FP32-accumulate filter + exact recheck */
+
+typedef struct hj_index hj_index;
+typedef struct hj_result hj_result;
+
+/* Layout of gridCellLookup in the reference (structs.h:90-98): 16 bytes. */
+typedef struct {
+    uint32_t idx;
+    uint32_t pad_;
+    uint64_t gridLinearID;
+} hj_grid_cell_lookup;
+
+/* Layout of grid (structs.h:83-86): inclusive [indexmin, indexmax]. */
+typedef struct {
+    int32_t indexmin;
+    int32_t indexmax;
+} hj_grid;
+
+/* Layout of schedulingCell (structs.h:101-104). */
+typedef struct {
+    int32_t nbPoints;
+    int32_t cellId;
+} hj_scheduling_cell;
+
+/* Device neighbour-table entry: the device form of neighborTableLookup
+ * (structs.h:35-41).  Query `q`'s neighbours are
+ * values[batch][start .. start + count). */
+typedef struct {
+    uint32_t batch;
+    uint32_t count;
+    uint64_t start;
+} hj_nt_entry;
+
+typedef struct {
+    uint32_t n, d, k, dtype;
+    uint32_t n_nonempty_cells;
+    uint32_t grid_aliasing;        /* 1 if some point's cell coordinate reached nCells */
+    uint64_t total_cells;
+    uint64_t total_candidates;     /* valid after hj_sort_by_workload */
+    double eps;                    /* epsilon in the dataset type */
+    double sq_threshold;           /* largest d2 with RN(sqrt(d2)) <= eps, dataset type */
+    double min_arr[16];
+    uint32_t n_cells[16];
+} hj_index_info;
+
+typedef struct {
+    int refine;                    /* HJ_REFINE_* */
+    uint64_t result_capacity;      /* pairs per batch buffer; 0 = from the estimate */
+    double sample_rate;            /* estimator sample rate; 0 = 0.02 */
+    double mem_fraction;           /* share of free device memory result buffers may use; 0 = 0.6 */
+    uint32_t query_block;          /* queries per work item; 0 = autotuned/default */
+    uint32_t max_batches;          /* safety cap on batch count; 0 = unlimited */
+    uint32_t use_graphs;           /* replay the per-batch sequence through a CUDA graph */
+    uint32_t keep_keys;            /* keep per-batch sorted key arrays (needed for the reference export) */
+} hj_join_opts;
+
+typedef struct {
+    uint64_t total_pairs;
+    uint32_t n_batches;
+    uint32_t n_retries;            /* batches re-run after an overflow */
+    uint64_t band_pairs;           /* tensor-core filter: pairs that needed the exact recheck */
+    uint64_t tc_accepts;           /* tensor-core filter: pairs accepted outside the band */
+    uint64_t estimated_pairs;      /* selectivity estimate before the join */
+    double filter_delta;           /* guard band half-width on d2 (tensor-core filter) */
+    float ms_estimate, ms_refine, ms_group, ms_total;
+    uint32_t refine_used;          /* HJ_REFINE_* actually used */
+    uint32_t kernel_launches;      /* kernels launched by this join */
+} hj_join_stats;
+
+/* ---- errors / library ---------------------------------------------------- */
+const char* hj_last_error(void);
+const char* hj_version(void);
+/* Kernels launched by this process so far (all entry points). */
+uint64_t hj_kernel_launch_count(void);
+
+/* ---- grid geometry: replaces generateNDGridDimensions (main.cu:449-520) ---- */
+/* Per indexed dimension: min/max over the points, widened by eps, nCells =
+ * ceil((max - min) / eps), all in the dataset type; min/max are reduced on the
+ * device.  Synchronises `stream`. */
+hj_status hj_grid_geometry(const void* d_db, uint32_t n, uint32_t d, uint32_t k, int dtype,
+                           double eps, double* h_min_arr, double* h_max_arr,
+                           uint32_t* h_n_cells, uint64_t* h_total_cells, void* stream);
+
+/* ---- index build: replaces gridIndexingGPU (GPU.cu:74-398, GPU.h:9-27) ----- */
+/* d_db: n x d row-major dataset on the device (float or double per dtype).
+ * h_min_arr / h_n_cells: the grid geometry (k entries); NULL = compute it with
+ * hj_grid_geometry.  Synchronises `stream`. */
+hj_status hj_index_create(const void* d_db, uint32_t n, uint32_t d, uint32_t k, int dtype,
+                          double eps, const double* h_min_arr, const uint32_t* h_n_cells,
+                          void* stream, hj_index** out);
+hj_status hj_index_destroy(hj_index* ix);
+hj_status hj_index_get_info(const hj_index* ix, hj_index_info* out);
+/* Write the reference's index arrays into caller buffers (device pointers;
+ * any may be NULL): gridCellLookupArr (nNonEmpty), index (nNonEmpty),
+ * indexLookupArr (n).  Enqueued on `stream`. */
+hj_status hj_index_export(const hj_index* ix, hj_grid_cell_lookup* d_lookup, hj_grid* d_grid,
+                          uint32_t* d_index_lookup, void* stream);
+/* Device views of the index: the points reordered by cell (n x d, dataset
+ * type), sorted-position -> original id, cell linear ids and cell starts
+ * (nNonEmpty + 1 entries). */
+hj_status hj_index_views(const hj_index* ix, const void** d_points_sorted, const uint32_t** d_perm,
+                         const uint64_t** d_cell_lid, const uint32_t** d_cell_start);
+
+/* ---- workload order: replaces sortByWorkLoad (SortByWorkload.cu:19-247) ---- */
+/* Candidate count per non-empty cell (summed populations of its 3^k stencil),
+ * cells ordered heaviest first (stable among equals), totalCandidates.
+ * Synchronises `stream`. */
+hj_status hj_sort_by_workload(hj_index* ix, void* stream, uint64_t* total_candidates);
+/* Export the ordered schedulingCell array (nNonEmpty) and originPointIndex (n)
+ * to device buffers (either may be NULL). */
+hj_status hj_workload_export(const hj_index* ix, hj_scheduling_cell* d_sched,
+                             uint32_t* d_origin_point_index, void* stream);
+
+/* ---- join: replaces distanceTableNDGridBatches (GPU.cu:787-1702) ---------- */
+void hj_join_opts_default(hj_join_opts* o);
+/* Runs estimator, batches, refine and result grouping.  The result keeps, per
+ * batch, the neighbour ids grouped by query (device memory) plus a device
+ * neighbour table of n entries.  Synchronises `stream`. */
+hj_status hj_join(hj_index* ix, const hj_join_opts* opts, void* stream, hj_result** out,
+                  hj_join_stats* stats);
+hj_status hj_result_destroy(hj_result* r);
+hj_status hj_result_num_batches(const hj_result* r, uint32_t* n_batches, uint64_t* total_pairs);
+/* Batch b: device pointers to its values (and keys when keep_keys was set),
+ * grouped by query id, and its pair count. */
+hj_status hj_result_batch(const hj_result* r, uint32_t b, const uint32_t** d_vals,
+                          const uint32_t** d_keys, uint64_t* count);
+/* Device neighbour table (n entries, indexed by original query id). */
+hj_status hj_result_table(const hj_result* r, const hj_nt_entry** d_table);
+/* Per-query CSR by original id into caller buffers: d_offsets (n + 1, u64) and
+ * d_vals (total_pairs, u32); neighbours of a query in ascending id order when
+ * sort_lists is set.  Enqueued on `stream`. */
+hj_status hj_result_to_csr(const hj_result* r, uint64_t* d_offsets, uint32_t* d_vals, int sort_lists,
+                           void* stream);
+/* Per-query order-independent digest (count, sum of mix64(id), xor of
+ * mix64(id ^ salt)) into device buffers of n entries. */
+hj_status hj_result_digest(const hj_result* r, uint32_t* d_count, uint64_t* d_sum, uint64_t* d_xor,
+                           void* stream);
+
+/* ---- one-shot convenience: host buffers in, host pair count out ------------ */
+/* Copies the dataset to the device, builds the index, sorts by workload and
+ * joins; the result stays on the device in *out (may be NULL to discard). */
+hj_status hj_self_join_host(const void* h_db, uint32_t n, uint32_t d, uint32_t k, int dtype, double eps,
+                            const hj_join_opts* opts, void* stream, hj_result** out,
+                            hj_join_stats* stats);
+
+/* ---- probes --------------------------------------------------------------- */
+/* Evaluates the reference's squared-distance expression (kernel.cu:350-353)
+ * as nvcc compiles it by default, for n pairs of d-dimensional rows; writes
+ * d2 per pair.  Used to establish the FMA contraction the reference gets. */
+hj_status hj_probe_sqdist(const void* d_a, const void* d_b, uint32_t n, uint32_t d, int dtype,
+                          void* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HEGJOIN_B200_H */
