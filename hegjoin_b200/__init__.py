@@ -58,14 +58,16 @@ class IndexInfo(ctypes.Structure):
 class JoinOpts(ctypes.Structure):
     _fields_ = [("refine", ctypes.c_int), ("result_capacity", ctypes.c_uint64), ("sample_rate", ctypes.c_double),
                 ("mem_fraction", ctypes.c_double), ("query_block", ctypes.c_uint32), ("max_batches", ctypes.c_uint32),
-                ("use_graphs", ctypes.c_uint32), ("keep_keys", ctypes.c_uint32)]
+                ("use_graphs", ctypes.c_uint32), ("keep_keys", ctypes.c_uint32), ("shard_count", ctypes.c_uint32),
+                ("shard_index", ctypes.c_uint32)]
 
 
 class JoinStats(ctypes.Structure):
     _fields_ = [("total_pairs", ctypes.c_uint64), ("n_batches", ctypes.c_uint32), ("n_retries", ctypes.c_uint32),
                 ("band_pairs", ctypes.c_uint64), ("tc_accepts", ctypes.c_uint64), ("estimated_pairs", ctypes.c_uint64),
                 ("filter_delta", ctypes.c_double), ("ms_estimate", ctypes.c_float), ("ms_refine", ctypes.c_float),
-                ("ms_group", ctypes.c_float), ("ms_total", ctypes.c_float), ("refine_used", ctypes.c_uint32),
+                ("ms_group", ctypes.c_float), ("ms_total", ctypes.c_float), ("ms_refine_kernel", ctypes.c_float),
+                ("refine_launches", ctypes.c_uint32), ("refine_used", ctypes.c_uint32),
                 ("kernel_launches", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
@@ -100,6 +102,7 @@ def _load() -> ctypes.CDLL:
         "hj_result_digest": (I, [P, P, P, P, P]),
         "hj_self_join_host": (I, [P, U32, U32, U32, I, D, P, P, P, P]),
         "hj_probe_sqdist": (I, [P, P, U32, U32, I, P, P]),
+        "hj_probe_tc_tile": (I, [P, I, U32, U32, P, P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -286,7 +289,7 @@ class JoinResult:
 
 
 def join_opts(refine="auto", result_capacity=0, sample_rate=0.0, mem_fraction=0.0, max_batches=0,
-              use_graphs=False, keep_keys=False) -> JoinOpts:
+              use_graphs=False, keep_keys=False, shard_count=0, shard_index=0) -> JoinOpts:
     o = JoinOpts()
     lib.hj_join_opts_default(ctypes.byref(o))
     o.refine = REFINE_NAMES[refine] if isinstance(refine, str) else int(refine)
@@ -298,6 +301,8 @@ def join_opts(refine="auto", result_capacity=0, sample_rate=0.0, mem_fraction=0.
     o.max_batches = int(max_batches)
     o.use_graphs = int(bool(use_graphs))
     o.keep_keys = int(bool(keep_keys))
+    o.shard_count = int(shard_count)
+    o.shard_index = int(shard_index)
     return o
 
 
@@ -343,3 +348,28 @@ def probe_sqdist(a, b, stream=None):
     out = torch.empty(n, dtype=a.dtype, device=a.device)
     check(lib.hj_probe_sqdist(_ptr(a), _ptr(b), n, d, _dtype_code(a), _ptr(out), _stream_ptr(stream)))
     return out
+
+
+def kpad_for(d: int) -> int:
+    return ((d + 4 + 31) // 32) * 32
+
+
+def probe_tc_tile(index: GridIndex, refine: str, a0: int, b0: int, stream=None):
+    """One candidate tile x 512 queries through the tensor-core path.
+
+    Returns (accumulators [128, 512] float32 numpy, query-form rows [512, kpad],
+    candidate-form rows [128, kpad]) with the operand rows as float64.
+    """
+    torch = _torch()
+    inf = index.info()
+    kp = kpad_for(inf.d)
+    out = torch.empty((128, 512), dtype=torch.float32, device=index.db.device)
+    hq = np.zeros((512, kp), np.uint16)
+    hc = np.zeros((128, kp), np.uint16)
+    check(lib.hj_probe_tc_tile(index.handle, REFINE_NAMES[refine], a0, b0, _ptr(out), hq.ctypes.data,
+                               hc.ctypes.data, _stream_ptr(stream)))
+    if refine == "tc_bf16":
+        conv = lambda a: (a.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+    else:
+        conv = lambda a: a.view(np.float16).astype(np.float64)
+    return out.cpu().numpy(), conv(hq), conv(hc)

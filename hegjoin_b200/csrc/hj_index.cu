@@ -36,6 +36,19 @@ uint64_t& launch_counter() {
     return c;
 }
 
+void init_memory_pool() {
+    static bool done = false;
+    if (done) return;
+    done = true;
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+}
+
 template <typename T>
 static T sq_threshold_t(T eps) {
     // sqrt is correctly rounded and monotone, so {x : RN(sqrt(x)) <= eps} is
@@ -379,6 +392,7 @@ hj_status index_create_t(const T* d_db, uint32_t n, uint32_t d, uint32_t k, T ep
 }
 
 void free_index(hj_index* ix, cudaStream_t st) {
+    tc_release(ix);
     dfree(ix->pts, st);
     dfree(ix->perm, st);
     dfree(ix->cell_lid, st);
@@ -463,6 +477,7 @@ hj_status hj_index_create(const void* d_db, uint32_t n, uint32_t d, uint32_t k, 
         if (tot > ~0ull / h_n_cells[j]) { set_error("hj_index_create: totalCells overflows 64 bits"); return HJ_ERR_UNSUPPORTED; }
         tot *= h_n_cells[j];
     }
+    init_memory_pool();
     hj_index* ix = new hj_index();
     ix->dtype = dtype;
     cudaGetDevice(&ix->device);

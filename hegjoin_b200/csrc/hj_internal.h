@@ -50,12 +50,19 @@ struct hj_index {
     float* tc_err = nullptr;         // per sorted point: quantisation error norm (rounded up)
     uint32_t tc_kpad = 0;
     int tc_kind = -1;                // HJ_REFINE_TC_F16 / _BF16 the operands hold
+    void* tc_state = nullptr;        // tensor maps and error maxima (hj_refine_tc.cu)
 };
 
 namespace hj {
 
 // Host: largest value x of the dataset type with RN(sqrt(x)) <= eps.
 double sq_threshold(double eps, int dtype);
+
+// Keep freed stream-ordered allocations mapped for reuse (called once per process).
+void init_memory_pool();
+
+// hj_refine_tc.cu
+void tc_release(hj_index* ix);
 
 // hj_index.cu
 hj_status build_blocks(const hj_index* ix, uint32_t qb, HjBlock** d_blocks, uint32_t* n_blocks,

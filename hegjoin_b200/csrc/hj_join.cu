@@ -35,8 +35,12 @@ hj_status launch_refine_plain(const hj_index* ix, const HjBlock* blocks, uint32_
 hj_status tc_prepare(hj_index* ix, int kind, cudaStream_t st);
 uint32_t tc_query_block();
 hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t nblocks, unsigned int* head,
-                           const PairSink& sink, uint32_t count_only, unsigned long long* block_counts,
-                           double delta, unsigned long long* stat_counters, cudaStream_t st);
+                           const PairSink& sink, const PairSink& band, uint32_t count_only,
+                           unsigned long long* block_counts, unsigned long long* stats, uint32_t* err,
+                           cudaStream_t st);
+hj_status launch_band_recheck(const hj_index* ix, const uint32_t* bq, const uint32_t* bc,
+                              const unsigned long long* band_used, unsigned long long band_cap,
+                              const PairSink& sink, cudaStream_t st);
 double tc_delta(const hj_index* ix);
 bool tc_supported(const hj_index* ix, int kind);
 }  // namespace hj
@@ -59,6 +63,12 @@ __global__ void k_pick_samples(const HjBlock* __restrict__ blocks, uint32_t nblo
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nsamp) return;
     out[i] = blocks[min(nblocks - 1, i * stride)];
+}
+
+__global__ void k_pick_strided(const HjBlock* __restrict__ blocks, uint32_t first, uint32_t stride, uint32_t m,
+                               HjBlock* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = blocks[first + i * stride];
 }
 
 // Number of non-sentinel keys in a sorted key array (sentinels sort last).
@@ -217,20 +227,61 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     HjBlock* blocks = nullptr;
     uint32_t nblocks = 0;
     HJ_TRY(build_blocks(ix, qb, &blocks, &nblocks, st));
+    if (opts.shard_count > 1) {
+        // this rank's share of the heaviest-first order: items i = shard_index mod shard_count
+        if (opts.shard_index >= opts.shard_count) { set_error("hj_join: shard_index >= shard_count"); return HJ_ERR_INVALID; }
+        uint32_t mine = nblocks > opts.shard_index ? (nblocks - opts.shard_index + opts.shard_count - 1) / opts.shard_count : 0;
+        HjBlock* sel = nullptr;
+        HJ_TRY(dalloc(&sel, std::max<uint32_t>(mine, 1), st));
+        if (mine) {
+            k_pick_strided<<<(mine + 255) / 256, 256, 0, st>>>(blocks, opts.shard_index, opts.shard_count, mine, sel);
+            HJ_LAUNCHED();
+        }
+        dfree(blocks, st);
+        blocks = sel;
+        nblocks = mine;
+    }
 
     unsigned int* head = nullptr;
-    unsigned long long* counters = nullptr;   // [0] cursor, [1] valid count, [2..5] tc stats
-    uint32_t* overflow = nullptr;
+    // [0] pair cursor, [1] valid count, [2] tc accepts, [3] tc band pairs, [4] band cursor
+    unsigned long long* counters = nullptr;
+    uint32_t* flags = nullptr;                 // [0] overflow, [1] bounded-wait timeout
     HJ_TRY(dalloc(&head, 1, st));
     HJ_TRY(dalloc(&counters, 8, st));
-    HJ_TRY(dalloc(&overflow, 1, st));
+    HJ_TRY(dalloc(&flags, 2, st));
     HJ_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
+    HJ_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), st));
+    uint32_t* overflow = flags;
+    PairSink no_band{nullptr, nullptr, nullptr, 0, overflow};
 
-    auto run_refine = [&](const HjBlock* blk, uint32_t nb, const PairSink& sink, uint32_t count_only,
-                          unsigned long long* bc) -> hj_status {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kev;   // refine kernel launches of the join proper
+    auto run_refine = [&](const HjBlock* blk, uint32_t nb, const PairSink& sink, const PairSink& band,
+                          uint32_t count_only, unsigned long long* bc) -> hj_status {
         HJ_CUDA(cudaMemsetAsync(head, 0, sizeof(unsigned int), st));
-        if (tc) return launch_refine_tc(ix, blk, nb, head, sink, count_only, bc, S.filter_delta, counters + 2, st);
-        return launch_refine_plain(ix, blk, nb, head, sink, count_only, bc, st);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (!count_only) {
+            HJ_CUDA(cudaEventCreate(&e0));
+            HJ_CUDA(cudaEventCreate(&e1));
+            HJ_CUDA(cudaEventRecord(e0, st));
+        }
+        hj_status r = tc ? launch_refine_tc(ix, blk, nb, head, sink, band, count_only, bc,
+                                            count_only ? nullptr : counters + 2, flags + 1, st)
+                         : launch_refine_plain(ix, blk, nb, head, sink, count_only, bc, st);
+        if (!count_only) {
+            HJ_CUDA(cudaEventRecord(e1, st));
+            kev.emplace_back(e0, e1);
+        }
+        return r;
+    };
+    auto check_timeout = [&]() -> hj_status {
+        uint32_t to = 0;
+        HJ_CUDA(cudaMemcpyAsync(&to, flags + 1, 4, cudaMemcpyDeviceToHost, st));
+        HJ_CUDA(cudaStreamSynchronize(st));
+        if (to) {
+            set_error("hj_join: a bounded device-side wait expired in the tensor-core pipeline");
+            return HJ_ERR_TIMEOUT;
+        }
+        return HJ_OK;
     };
 
     // ---- estimator (GPUBatchEst_v2, GPU.cu:403-779)
@@ -250,7 +301,8 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         k_pick_samples<<<(nsamp + 255) / 256, 256, 0, st>>>(blocks, nblocks, stride, nsamp, sblocks);
         HJ_LAUNCHED();
         PairSink none{nullptr, nullptr, nullptr, 0, overflow};
-        HJ_TRY(run_refine(sblocks, nsamp, none, 1, scnt));
+        HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
+        HJ_TRY(check_timeout());
         std::vector<unsigned long long> hs(nsamp);
         HJ_CUDA(cudaMemcpyAsync(hs.data(), scnt, nsamp * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
@@ -277,7 +329,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     size_t free_b = 0, total_b = 0;
     HJ_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const uint64_t chunk_slack = (uint64_t)num_sms() * 64 * kSinkChunk;   // partially filled warp chunks
-    const double bytes_per_slot = 16.0 + 4.0 + (opts.keep_keys ? 4.0 : 0.0);
+    const double bytes_per_slot = 16.0 + 4.0 + (opts.keep_keys ? 4.0 : 0.0) + (tc ? 8.0 : 0.0);
     uint64_t max_cap = (uint64_t)(opts.mem_fraction * (double)free_b / bytes_per_slot);
     max_cap = std::min<uint64_t>(max_cap, 0xF0000000ull);
     uint64_t want = (uint64_t)(total_est * 2.0) + chunk_slack + 4096;
@@ -307,10 +359,15 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     std::reverse(batches.begin(), batches.end());   // used as a stack
 
     uint32_t *keys = nullptr, *vals = nullptr, *keys_tmp = nullptr, *vals_tmp = nullptr;
+    uint32_t *band_q = nullptr, *band_c = nullptr;
     HJ_TRY(dalloc(&keys, cap, st));
     HJ_TRY(dalloc(&vals, cap, st));
     HJ_TRY(dalloc(&keys_tmp, cap, st));
     HJ_TRY(dalloc(&vals_tmp, cap, st));
+    if (tc) {
+        HJ_TRY(dalloc(&band_q, cap, st));
+        HJ_TRY(dalloc(&band_c, cap, st));
+    }
 
     hj_result* res = new hj_result();
     res->n = ix->n;
@@ -331,10 +388,18 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
             break;
         }
         HJ_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st));
+        HJ_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), st));
         HJ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(uint32_t), st));
         PairSink sink{keys, vals, counters, cap, overflow};
-        status = run_refine(blocks + b.b0, b.b1 - b.b0, sink, 0, nullptr);
+        PairSink band = tc ? PairSink{band_q, band_c, counters + 4, cap, overflow} : no_band;
+        status = run_refine(blocks + b.b0, b.b1 - b.b0, sink, band, 0, nullptr);
         if (status != HJ_OK) break;
+        if (tc) {
+            status = launch_band_recheck(ix, band_q, band_c, counters + 4, cap, sink, st);
+            if (status != HJ_OK) break;
+            status = check_timeout();
+            if (status != HJ_OK) break;
+        }
         unsigned long long used = 0;
         uint32_t ovf = 0;
         HJ_CUDA(cudaMemcpyAsync(&used, counters, 8, cudaMemcpyDeviceToHost, st));
@@ -388,6 +453,14 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     HJ_CUDA(cudaStreamSynchronize(st));
     S.ms_refine = ms_since(t_ref) - ms_group;
     S.ms_group = ms_group;
+    for (auto& ev : kev) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ev.first, ev.second) == cudaSuccess) S.ms_refine_kernel += ms;
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+        S.refine_launches++;
+    }
+    cudaGetLastError();
     if (tc) {
         unsigned long long tcs[2] = {0, 0};
         HJ_CUDA(cudaMemcpy(tcs, counters + 2, sizeof(tcs), cudaMemcpyDeviceToHost));
@@ -395,7 +468,8 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         S.band_pairs = tcs[1];
     }
     dfree(keys, st); dfree(vals, st); dfree(keys_tmp, st); dfree(vals_tmp, st);
-    dfree(blocks, st); dfree(head, st); dfree(counters, st); dfree(overflow, st);
+    dfree(band_q, st); dfree(band_c, st);
+    dfree(blocks, st); dfree(head, st); dfree(counters, st); dfree(flags, st);
     if (status == HJ_OK && !res->vals.empty()) {
         hj_status s2 = dalloc(&res->d_batch_vals, res->vals.size(), st);
         if (s2 == HJ_OK)

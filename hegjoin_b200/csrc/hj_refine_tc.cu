@@ -1,17 +1,809 @@
-// hj_refine_tc.cu -- tensor-core distance filter (placeholder until the tcgen05 kernel lands).
+// hj_refine_tc.cu -- tensor-core squared-distance filter with exact recheck.
+//
+// Reference counterpart: the refine kernelNDGridIndexGlobal (kernel.cu:727-802,
+// evalPoint kernel.cu:333-370).  For high dimensions the reference's candidate
+// loop is a dense distance evaluation; here each (candidate tile x query block)
+// is a GEMM on the 5th-generation tensor cores:
+//
+//   A (M = 128 candidates, streamed by TMA) = [-2 c~, 1, 1, |c~|^2_hi, |c~|^2_lo, 0...]
+//   B (N = 4 x 128 queries, resident)       = [  q~, |q~|^2_hi, |q~|^2_lo, 1, 1, 0...]
+//   D = A B^T = |q~|^2 + |c~|^2 - 2 q~.c~ = |q~ - c~|^2        (FP32 accumulate in TMEM)
+//
+// where x~ is the FP16 (or BF16) rounding of x - origin.  The norms ride in the
+// K padding (d + 4 rounded up to 32), so the MMA yields the squared distance
+// directly and the epilogue is one compare per pair.  A pair is
+//   accepted  if D <= T - delta,
+//   rejected  if D >  T + delta,
+//   rechecked otherwise, in FP32 in the reference's order (fma chain),
+// with T the exact squared threshold and delta a per-candidate-row bound on
+// |D - d2_ref| (quantisation error, norm-split residual, tensor-core
+// accumulation error and the reference's own FP32 rounding; derivation in
+// tc_delta_row below).  The result set is therefore identical to the exact path.
+//
+// Kernel shape (one CTA per SM, persistent, 192 threads):
+//   warp 0      TMA producer: query tiles once per work item, candidate tiles
+//               through a ring of shared-memory stages;
+//   warp 1      MMA issuer: per candidate tile, 4 MMAs (one per query tile) into
+//               4 TMEM accumulators of 128 columns (all 512 TMEM columns);
+//   warps 2..5  epilogue: tcgen05.ld 32 columns at a time, min-reduce, compare,
+//               warp-aggregated emission; releases an accumulator as soon as it
+//               has been read, so MMA and epilogue overlap across accumulators.
+// Every wait is bounded; a timeout raises an error flag, drains and returns.
+
+#include <cudaTypedefs.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+
 #include "hj_internal.h"
+#include "hj_tc.cuh"
 
 namespace hj {
-bool tc_supported(const hj_index*, int) { return false; }
-uint32_t tc_query_block() { return 512; }
-double tc_delta(const hj_index*) { return 0.0; }
-hj_status tc_prepare(hj_index*, int, cudaStream_t) {
-    set_error("tensor-core filter not built");
-    return HJ_ERR_UNSUPPORTED;
+namespace {
+
+constexpr int kQT = 4;                       // query tiles per work item
+constexpr int kTileRows = 128;               // rows per tile (M for A, N for B)
+constexpr int kQB = kQT * kTileRows;         // queries per work item
+constexpr int kThreads = 192;
+constexpr int kMaxStages = 8;
+constexpr uint32_t kKBlockBytes = kTileRows * 64;   // one 32-element K block of a tile
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kMaxRanges = 256;
+constexpr long long kWaitCycles = 4000000000ll;     // ~2 s at 1.9 GHz
+
+struct TcArgs {
+    const HjBlock* blocks;
+    uint32_t nblocks;
+    unsigned int* head;
+    const uint32_t* perm;
+    const unsigned long long* cell_lid;
+    const uint32_t* cell_start;
+    uint32_t nC;
+    HjGrid grid;
+    const float4* pinfo;        // per sorted point: quantisation error norm, |x~|^2, norm-split residual
+    uint32_t n;
+    uint32_t nkb;               // K blocks of 32 elements
+    uint32_t stages;
+    float thr;
+    float gamma_acc;
+    float s_t;                  // sqrt(T (1 + 1e-4))
+    float ref_rel;              // (d + 2) 2^-24 (1.01)
+    PairSink sink;              // accepted pairs: (query id, candidate id)
+    PairSink band;              // band pairs: (query sorted position, candidate sorted position)
+    uint32_t count_only;
+    unsigned long long* block_counts;
+    unsigned long long* stats;  // [0] accepted, [1] band
+    uint32_t* err;
+    uint32_t idesc;
+};
+
+struct TcShared {
+    uint64_t full_a[kMaxStages];
+    uint64_t empty_a[kMaxStages];
+    uint64_t full_acc[kQT];
+    uint64_t empty_acc[kQT];
+    uint64_t bfull;
+    uint32_t tmem_base;
+    uint32_t item;
+    uint32_t abort;
+    uint32_t nq, nqt, ntiles, nr, q0;
+    uint32_t max_e, max_n, max_r;          // float bits (non-negative)
+    uint32_t qid[kQB];
+    uint32_t rs[kMaxRanges];               // range start (sorted position)
+    uint32_t rl[kMaxRanges];               // range length
+    uint32_t tp[kMaxRanges + 1];           // tile prefix
+};
+
+__device__ __forceinline__ uint32_t lower_bound_lid(const unsigned long long* a, uint32_t n, unsigned long long v) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
 }
-hj_status launch_refine_tc(const hj_index*, const HjBlock*, uint32_t, unsigned int*, const PairSink&, uint32_t,
-                           unsigned long long*, double, unsigned long long*, cudaStream_t) {
-    set_error("tensor-core filter not built");
-    return HJ_ERR_UNSUPPORTED;
+
+__device__ __forceinline__ uint32_t tile_range(const TcShared& S, uint32_t t) {
+    uint32_t lo = 0, hi = S.nr;   // last r with tp[r] <= t
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (S.tp[mid] <= t) lo = mid; else hi = mid;
+    }
+    return lo;
 }
+
+__device__ __forceinline__ float min3f(float a, float b, float c) { return fminf(fminf(a, b), c); }
+
+// delta for one candidate row against the whole query block (all bounds rounded up):
+//   |D - d2_ref| <= acc + res + e (2 sT + 3 e) + ref_rel (sT + e)^2
+//   e   = e_c + max e_q       (|x~ - x| norms; |(|q~-c~|) - |q-c|| <= e)
+//   acc = gamma (2.01 (|c~|^2 + max |q~|^2))   (tensor-core accumulation; 2|a.b| <= |a|^2 + |b|^2)
+//   res = r_c + max r_q       (norm split residuals)
+//   the last term bounds the reference's own FP32 rounding of d2 (d + 2 roundings)
+__device__ __forceinline__ float tc_delta_row(const TcArgs& a, float4 pc, float me, float mn, float mr) {
+    float e = pc.x + me;
+    float acc = a.gamma_acc * 2.01f * (pc.y + mn);
+    float r = pc.z + mr;
+    float ste = a.s_t + e;
+    float d = acc + r + e * (2.0f * a.s_t + 3.0f * e) + a.ref_rel * ste * ste;
+    return d * 1.01f + 1e-30f;
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_refine_tc(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query, TcArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    // operand tiles need 1024-byte alignment for the swizzle pattern
+    uint32_t base = tc::smem_u32(smem_raw);
+    uint8_t* smem = smem_raw + ((1024u - (base & 1023u)) & 1023u);
+    const uint32_t tile_bytes = a.nkb * kKBlockBytes;
+    uint8_t* b_tiles = smem;                                   // kQT tiles
+    uint8_t* a_tiles = smem + kQT * tile_bytes;                // a.stages tiles
+    TcShared& S = *reinterpret_cast<TcShared*>(a_tiles + a.stages * tile_bytes);
+
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    if (tid == 0) {
+        for (uint32_t s = 0; s < a.stages; ++s) {
+            tc::mbar_init(&S.full_a[s], 1);
+            tc::mbar_init(&S.empty_a[s], 1);
+        }
+        for (int j = 0; j < kQT; ++j) {
+            tc::mbar_init(&S.full_acc[j], 1);
+            tc::mbar_init(&S.empty_acc[j], 4);
+        }
+        tc::mbar_init(&S.bfull, 1);
+        S.abort = 0;
+        tc::fence_mbar_init();
+        tc::tma_prefetch_desc(&tm_cand);
+        tc::tma_prefetch_desc(&tm_query);
+    }
+    if (warp == 1) {
+        tc::tmem_alloc(&S.tmem_base, kTmemCols);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = S.tmem_base;
+    volatile uint32_t* abort = &S.abort;
+
+    // role state carried across work items (barrier phases)
+    uint32_t it = 0;            // candidate tiles issued / consumed
+    uint32_t acc_use[kQT] = {0, 0, 0, 0};
+    uint32_t items_loaded = 0;
+    WarpChunk wc_acc, wc_band;
+    warp_chunk_init(wc_acc);
+    warp_chunk_init(wc_band);
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) {
+            S.item = *abort ? 0xFFFFFFFFu : atomicAdd(a.head, 1u);
+            S.max_e = S.max_n = S.max_r = 0u;
+        }
+        __syncthreads();
+        const uint32_t item = S.item;
+        if (item >= a.nblocks) break;
+        const HjBlock blk = a.blocks[item];
+        const uint32_t nq = blk.q1 - blk.q0;
+        // query ids and block maxima of the error terms
+        {
+            float me = 0.f, mn = 0.f, mr = 0.f;
+            for (uint32_t i = tid; i < (uint32_t)kQB; i += kThreads) {
+                S.qid[i] = i < nq ? a.perm[blk.q0 + i] : 0u;
+                if (i < nq) {
+                    float4 p = a.pinfo[blk.q0 + i];
+                    me = fmaxf(me, p.x); mn = fmaxf(mn, p.y); mr = fmaxf(mr, p.z);
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                me = fmaxf(me, __shfl_xor_sync(0xffffffffu, me, o));
+                mn = fmaxf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+            }
+            if (lane == 0) {
+                atomicMax(&S.max_e, __float_as_uint(me));
+                atomicMax(&S.max_n, __float_as_uint(mn));
+                atomicMax(&S.max_r, __float_as_uint(mr));
+            }
+        }
+        if (warp == 0) {
+            // stencil rows of the block's cell -> candidate ranges -> 128-row tiles
+            const unsigned long long L = a.cell_lid[blk.cell];
+            const uint32_t k = a.grid.k;
+            uint32_t lo[kMaxK], w[kMaxK];
+            uint32_t rows = 1;
+            bool empty = false;
+            for (uint32_t j = 0; j < k; ++j) {
+                uint32_t c = (j + 1 < k) ? (uint32_t)((L / a.grid.mult[j]) % a.grid.n_cells[j])
+                                         : (uint32_t)(L / a.grid.mult[j]);
+                uint32_t l = c - 1u;                                // kernel.cu:780, wraps at 0
+                uint32_t h = min(a.grid.n_cells[j] - 1u, c + 1u);   // kernel.cu:781
+                empty |= l > h;
+                lo[j] = l;
+                w[j] = h - l + 1u;
+                if (j > 0) rows *= w[j];
+            }
+            if (empty) rows = 0;
+            uint32_t tiles_mine[kMaxRanges / 32];
+            uint32_t my_tiles = 0;
+#pragma unroll
+            for (uint32_t s = 0; s < kMaxRanges / 32; ++s) {
+                uint32_t r = lane * (kMaxRanges / 32) + s;
+                uint32_t len = 0, st = 0;
+                if (r < rows) {
+                    uint32_t rem = r;
+                    unsigned long long bse = 0;
+                    for (uint32_t j = 1; j < k; ++j) {
+                        uint32_t t = lo[j] + rem % w[j];
+                        rem /= w[j];
+                        bse += (unsigned long long)t * a.grid.mult[j];
+                    }
+                    unsigned long long la = bse + lo[0], lb = la + w[0] - 1;
+                    uint32_t c0 = lower_bound_lid(a.cell_lid, a.nC, la), c1 = c0;
+                    while (c1 < a.nC && a.cell_lid[c1] <= lb) ++c1;
+                    st = a.cell_start[c0];
+                    len = a.cell_start[c1] - st;
+                    S.rs[r] = st;
+                    S.rl[r] = len;
+                }
+                tiles_mine[s] = (len + kTileRows - 1) / kTileRows;
+                my_tiles += tiles_mine[s];
+            }
+            uint32_t incl = my_tiles;
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += t;
+            }
+            uint32_t run = incl - my_tiles;
+            const uint32_t nr = min(rows, kMaxRanges);
+#pragma unroll
+            for (uint32_t s = 0; s < kMaxRanges / 32; ++s) {
+                uint32_t r = lane * (kMaxRanges / 32) + s;
+                if (r < nr) S.tp[r] = run;
+                run += tiles_mine[s];
+            }
+            if (lane == 31) {
+                S.tp[nr] = incl;
+                S.ntiles = incl;
+                S.nr = nr;
+                S.nq = nq;
+                S.nqt = (nq + kTileRows - 1) / kTileRows;
+                S.q0 = blk.q0;
+            }
+        }
+        __syncthreads();
+        const uint32_t ntiles = S.ntiles, nqt = S.nqt;
+        if (ntiles == 0) continue;
+
+        if (warp == 0) {
+            if (lane == 0) {
+                // ---------------- TMA producer
+                tc::mbar_arrive_expect_tx(&S.bfull, nqt * tile_bytes);
+                for (uint32_t j = 0; j < nqt; ++j)
+                    for (uint32_t kb = 0; kb < a.nkb; ++kb)
+                        tc::tma_load_2d(b_tiles + j * tile_bytes + kb * kKBlockBytes, &tm_query, &S.bfull,
+                                        (int)(kb * 32), (int)(blk.q0 + j * kTileRows));
+                for (uint32_t t = 0; t < ntiles; ++t, ++it) {
+                    const uint32_t s = it % a.stages, use = it / a.stages;
+                    if (use > 0 && !tc::mbar_wait(&S.empty_a[s], (use - 1) & 1u, abort, a.err, kWaitCycles)) break;
+                    const uint32_t r = tile_range(S, t);
+                    const uint32_t start = S.rs[r] + (t - S.tp[r]) * kTileRows;
+                    tc::mbar_arrive_expect_tx(&S.full_a[s], tile_bytes);
+                    for (uint32_t kb = 0; kb < a.nkb; ++kb)
+                        tc::tma_load_2d(a_tiles + s * tile_bytes + kb * kKBlockBytes, &tm_cand, &S.full_a[s],
+                                        (int)(kb * 32), (int)start);
+                }
+            }
+            __syncwarp();
+            it = __shfl_sync(0xffffffffu, it, 0);
+        } else if (warp == 1) {
+            if (lane == 0) {
+                // ---------------- MMA issuer
+                bool ok = tc::mbar_wait(&S.bfull, items_loaded & 1u, abort, a.err, kWaitCycles);
+                tc::fence_after();
+                const uint32_t ksteps = a.nkb * 2;
+                const uint32_t a_base = tc::smem_u32(a_tiles), b_base = tc::smem_u32(b_tiles);
+                for (uint32_t t = 0; ok && t < ntiles; ++t, ++it) {
+                    const uint32_t s = it % a.stages, use = it / a.stages;
+                    if (!tc::mbar_wait(&S.full_a[s], use & 1u, abort, a.err, kWaitCycles)) break;
+                    tc::fence_after();
+                    for (uint32_t j = 0; j < nqt; ++j) {
+                        if (acc_use[j] > 0 &&
+                            !tc::mbar_wait(&S.empty_acc[j], (acc_use[j] - 1) & 1u, abort, a.err, kWaitCycles)) {
+                            ok = false;
+                            break;
+                        }
+                        tc::fence_after();
+                        for (uint32_t ks = 0; ks < ksteps; ++ks) {
+                            const uint32_t koff = (ks >> 1) * kKBlockBytes + (ks & 1u) * 32u;
+                            uint64_t ad = tc::desc_kmajor_sw64(a_base + s * tile_bytes + koff);
+                            uint64_t bd = tc::desc_kmajor_sw64(b_base + j * tile_bytes + koff);
+                            tc::mma_f16(tmem + j * kTileRows, ad, bd, a.idesc, ks > 0 ? 1u : 0u);
+                        }
+                        tc::mma_commit(&S.full_acc[j]);
+                        ++acc_use[j];
+                    }
+                    tc::mma_commit(&S.empty_a[s]);
+                }
+            }
+            __syncwarp();
+            it = __shfl_sync(0xffffffffu, it, 0);
+#pragma unroll
+            for (int j = 0; j < kQT; ++j) acc_use[j] = __shfl_sync(0xffffffffu, acc_use[j], 0);
+            ++items_loaded;
+        } else {
+            // ---------------- epilogue: warps 2..5, TMEM lane quarter = warp % 4
+            const uint32_t quarter = warp & 3u;
+            const uint32_t row = quarter * 32u + lane;
+            const float me = __uint_as_float(S.max_e), mn = __uint_as_float(S.max_n), mr = __uint_as_float(S.max_r);
+            unsigned long long n_acc = 0, n_band = 0;
+            bool ok = true;
+            for (uint32_t t = 0; ok && t < ntiles; ++t) {
+                const uint32_t r = tile_range(S, t);
+                const uint32_t off = (t - S.tp[r]) * kTileRows;
+                const uint32_t start = S.rs[r] + off;
+                const uint32_t valid = min((uint32_t)kTileRows, S.rl[r] - off);
+                const bool vrow = row < valid;
+                const uint32_t cpos = start + row;
+                float hi = -INFINITY, lo = -INFINITY;
+                if (vrow) {
+                    float d = tc_delta_row(a, a.pinfo[cpos], me, mn, mr);
+                    hi = __fadd_ru(a.thr, d);
+                    lo = __fsub_rd(a.thr, d);
+                }
+                uint32_t cid = 0xFFFFFFFFu;
+                for (uint32_t j = 0; j < nqt; ++j) {
+                    if (!tc::mbar_wait(&S.full_acc[j], acc_use[j] & 1u, abort, a.err, kWaitCycles)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after();
+                    const uint32_t ncols = min((uint32_t)kTileRows, nq - j * kTileRows);
+                    for (uint32_t c = 0; c < 4; ++c) {
+                        float v[32];
+                        tc::tmem_ld_32x32(tmem + ((quarter * 32u) << 16) + j * kTileRows + c * 32u, v);
+                        tc::tmem_ld_wait();
+                        if (c == 3) {
+                            // the accumulator has been read: hand it back to the MMA warp
+                            tc::fence_before();
+                            __syncwarp();
+                            if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
+                        }
+                        float m = v[0];
+#pragma unroll
+                        for (int i = 1; i < 31; i += 2) m = min3f(m, v[i], v[i + 1]);
+                        m = fminf(m, v[31]);
+                        const bool any_hit = m <= hi;
+                        if (!__any_sync(0xffffffffu, any_hit)) continue;
+                        uint32_t hmask = 0, amask = 0;
+                        const uint32_t cbase = c * 32u;
+                        if (any_hit) {
+#pragma unroll
+                            for (int i = 0; i < 32; ++i) {
+                                bool inq = cbase + i < ncols;
+                                hmask |= (uint32_t)(inq && v[i] <= hi) << i;
+                                amask |= (uint32_t)(inq && v[i] <= lo) << i;
+                            }
+                        }
+                        const uint32_t bmask = hmask & ~amask;
+                        n_acc += __popc(amask);
+                        n_band += __popc(bmask);
+                        if (a.count_only) continue;
+                        if (amask && cid == 0xFFFFFFFFu) cid = a.perm[cpos];
+                        const uint32_t qcol = j * kTileRows + cbase;
+                        uint32_t m1 = amask;
+                        warp_emit(a.sink, wc_acc, __popc(amask), [&](uint32_t) {
+                            uint32_t b = __ffs(m1) - 1;
+                            m1 &= m1 - 1;
+                            return make_uint2(S.qid[qcol + b], cid);
+                        });
+                        uint32_t m2 = bmask;
+                        const uint32_t q0 = S.q0;
+                        warp_emit(a.band, wc_band, __popc(bmask), [&](uint32_t) {
+                            uint32_t b = __ffs(m2) - 1;
+                            m2 &= m2 - 1;
+                            return make_uint2(q0 + qcol + b, cpos);
+                        });
+                    }
+                    ++acc_use[j];
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                n_acc += __shfl_down_sync(0xffffffffu, n_acc, o);
+                n_band += __shfl_down_sync(0xffffffffu, n_band, o);
+            }
+            if (lane == 0) {
+                if (a.count_only) {
+                    if (n_acc + n_band) atomicAdd(&a.block_counts[item], n_acc + n_band);
+                } else if (a.stats) {
+                    if (n_acc) atomicAdd(&a.stats[0], n_acc);
+                    if (n_band) atomicAdd(&a.stats[1], n_band);
+                }
+            }
+            it += ntiles;
+        }
+    }
+    if (warp >= 2 && !a.count_only) {
+        warp_chunk_close(a.sink, wc_acc);
+        warp_chunk_close(a.band, wc_band);
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::fence_after();
+        tc::tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+// Band pairs: exact FP32 refine in the reference's order (kernel.cu:350-355).
+__global__ void k_band_recheck(const float* __restrict__ pts, const uint32_t* __restrict__ perm, uint32_t d,
+                               float thr, const uint32_t* __restrict__ bq, const uint32_t* __restrict__ bc,
+                               const unsigned long long* __restrict__ band_used, unsigned long long band_cap,
+                               PairSink sink) {
+    const unsigned long long n = min(*band_used, band_cap);
+    WarpChunk wc;
+    warp_chunk_init(wc);
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+        unsigned long long i = base + threadIdx.x;
+        bool hit = false;
+        uint32_t qp = 0, cp = 0;
+        if (i < n) {
+            qp = bq[i];
+            if (qp != kSentinelKey) {
+                cp = bc[i];
+                const float* q = pts + (size_t)qp * d;
+                const float* c = pts + (size_t)cp * d;
+                float acc = 0.f;
+                for (uint32_t l = 0; l < d; ++l) {
+                    float diff = __fsub_rn(c[l], q[l]);
+                    acc = __fmaf_rn(diff, diff, acc);
+                }
+                hit = acc <= thr;
+            }
+        }
+        warp_emit(sink, wc, hit ? 1u : 0u, [&](uint32_t) { return make_uint2(perm[qp], perm[cp]); });
+    }
+    warp_chunk_close(sink, wc);
+}
+
+// Operand preparation: one thread per sorted point.
+template <typename H>
+__device__ __forceinline__ H to_h(double x);
+template <>
+__device__ __forceinline__ __half to_h<__half>(double x) { return __double2half(x); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 to_h<__nv_bfloat16>(double x) { return __double2bfloat16(x); }
+__device__ __forceinline__ double from_h(__half h) { return (double)__half2float(h); }
+__device__ __forceinline__ double from_h(__nv_bfloat16 h) { return (double)__bfloat162float(h); }
+
+template <typename H>
+__global__ void k_tc_prep(const float* __restrict__ pts, uint32_t n, uint32_t d, uint32_t kpad,
+                          const float* __restrict__ origin, H* __restrict__ qform, H* __restrict__ cform,
+                          float4* __restrict__ pinfo) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double n2 = 0, e2 = 0;
+    H* qr = qform + (size_t)i * kpad;
+    H* cr = cform + (size_t)i * kpad;
+    for (uint32_t l = 0; l < d; ++l) {
+        double x = (double)pts[(size_t)i * d + l] - (double)origin[l];
+        H h = to_h<H>(x);
+        double xt = from_h(h);
+        e2 += (xt - x) * (xt - x);
+        n2 += xt * xt;
+        qr[l] = h;
+        cr[l] = to_h<H>(-2.0 * xt);
+    }
+    H nh = to_h<H>(n2);
+    H nl = to_h<H>(n2 - from_h(nh));
+    double res = fabs(n2 - from_h(nh) - from_h(nl));
+    H one = to_h<H>(1.0), zero = to_h<H>(0.0);
+    qr[d] = nh; qr[d + 1] = nl; qr[d + 2] = one; qr[d + 3] = one;
+    cr[d] = one; cr[d + 1] = one; cr[d + 2] = nh; cr[d + 3] = nl;
+    for (uint32_t l = d + 4; l < kpad; ++l) { qr[l] = zero; cr[l] = zero; }
+    // round the bounds up: float conversion is to nearest, so scale by 1 + 2^-20
+    const float up = 1.0f + 9.6e-7f;
+    pinfo[i] = make_float4((float)sqrt(e2) * up, (float)n2 * up, (float)res * up + 1e-30f, 0.f);
+}
+
+__global__ void k_col_min(const float* __restrict__ pts, uint32_t n, uint32_t d, float* __restrict__ out) {
+    uint32_t l = blockIdx.x;
+    float m = INFINITY;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) m = fminf(m, pts[(size_t)i * d + l]);
+    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float w[32];
+    if (lane_id() == 0) w[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t k = 1; k < blockDim.x / 32; ++k) m = fminf(m, w[k]);
+        out[l] = fminf(m, w[0]);
+    }
+}
+
+// Debug/test kernel: one candidate tile (rows a0..a0+127) against four query
+// tiles (rows b0..b0+511) through the same TMA maps, descriptors and MMA
+// sequence as k_refine_tc; writes every accumulator value to out[128][512].
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tc_tile_probe(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query,
+                    uint32_t nkb, uint32_t idesc, uint32_t a0, uint32_t b0, float* __restrict__ out, uint32_t* err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint32_t base = tc::smem_u32(smem_raw);
+    uint8_t* smem = smem_raw + ((1024u - (base & 1023u)) & 1023u);
+    const uint32_t tile_bytes = nkb * kKBlockBytes;
+    uint8_t* b_tiles = smem;
+    uint8_t* a_tile = smem + kQT * tile_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(a_tile + tile_bytes);   // [0] loads, [1] mma
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+    uint32_t* abortp = tslot + 1;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    if (tid == 0) {
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
+        *abortp = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == 1) {
+        tc::tmem_alloc(tslot, kTmemCols);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tslot;
+    if (tid == 0) {
+        tc::mbar_arrive_expect_tx(&bars[0], (kQT + 1) * tile_bytes);
+        for (uint32_t kb = 0; kb < nkb; ++kb) {
+            tc::tma_load_2d(a_tile + kb * kKBlockBytes, &tm_cand, &bars[0], (int)(kb * 32), (int)a0);
+            for (uint32_t j = 0; j < kQT; ++j)
+                tc::tma_load_2d(b_tiles + j * tile_bytes + kb * kKBlockBytes, &tm_query, &bars[0], (int)(kb * 32),
+                                (int)(b0 + j * kTileRows));
+        }
+    }
+    if (tid == 32) {
+        bool ok = tc::mbar_wait(&bars[0], 0, abortp, err, kWaitCycles);
+        tc::fence_after();
+        if (ok) {
+            for (uint32_t j = 0; j < kQT; ++j)
+                for (uint32_t ks = 0; ks < nkb * 2; ++ks) {
+                    const uint32_t koff = (ks >> 1) * kKBlockBytes + (ks & 1u) * 32u;
+                    tc::mma_f16(tmem + j * kTileRows, tc::desc_kmajor_sw64(tc::smem_u32(a_tile) + koff),
+                                tc::desc_kmajor_sw64(tc::smem_u32(b_tiles) + j * tile_bytes + koff), idesc,
+                                ks > 0 ? 1u : 0u);
+                }
+        }
+        tc::mma_commit(&bars[1]);
+    }
+    if (warp >= 2) {
+        const uint32_t quarter = warp & 3u;
+        bool ok = tc::mbar_wait(&bars[1], 0, abortp, err, kWaitCycles);
+        tc::fence_after();
+        if (ok) {
+            for (uint32_t col = 0; col < (uint32_t)kQB; col += 32) {
+                float v[32];
+                tc::tmem_ld_32x32(tmem + ((quarter * 32u) << 16) + col, v);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int i = 0; i < 32; ++i) out[(size_t)(quarter * 32 + lane) * kQB + col + i] = v[i];
+            }
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::fence_after();
+        tc::tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+// ---- host side -------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+hj_status make_map(CUtensorMap* m, const void* base, uint32_t rows, uint32_t kpad, int kind) {
+    auto fn = encode_fn();
+    if (!fn) { set_error("cuTensorMapEncodeTiled is not available"); return HJ_ERR_CUDA; }
+    cuuint64_t dims[2] = {kpad, rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kpad * 2};
+    cuuint32_t box[2] = {32, (cuuint32_t)kTileRows};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = fn(m, kind == HJ_REFINE_TC_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                    2, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return HJ_ERR_CUDA;
+    }
+    return HJ_OK;
+}
+
+uint32_t kpad_for(uint32_t d) { return ((d + 4 + 31) / 32) * 32; }
+
+size_t tc_smem_bytes(uint32_t nkb, uint32_t stages) {
+    return 1024 + (size_t)(kQT + stages) * nkb * kKBlockBytes + sizeof(TcShared);
+}
+
+uint32_t tc_stages(uint32_t nkb) {
+    size_t budget = 225 * 1024;
+    uint32_t s = kMaxStages;
+    while (s > 2 && tc_smem_bytes(nkb, s) > budget) --s;
+    return s;
+}
+
+struct TcMaps {
+    CUtensorMap cand, query;
+};
+
+}  // namespace
+
+struct TcState {
+    TcMaps maps;
+    float gamma_acc = 0;
+    float max_e = 0, max_n = 0, max_r = 0;
+};
+
+static TcState* tc_state(const hj_index* ix) { return reinterpret_cast<TcState*>(ix->tc_state); }
+
+bool tc_supported(const hj_index* ix, int kind) {
+    if (ix->dtype != HJ_F32 || ix->d < 8) return false;
+    if (kind != HJ_REFINE_TC_F16 && kind != HJ_REFINE_TC_BF16) return false;
+    uint32_t nkb = kpad_for(ix->d) / 32;
+    if (tc_smem_bytes(nkb, 2) > 225 * 1024) return false;
+    uint32_t rows = 1;
+    for (uint32_t j = 1; j < ix->k; ++j) rows *= 3;
+    return rows <= kMaxRanges && ix->n < 0x7FFFFF00u;
+}
+
+uint32_t tc_query_block() { return kQB; }
+
+double tc_delta(const hj_index* ix) {
+    TcState* s = tc_state(ix);
+    if (!s) return 0;
+    double T = ix->thr, sT = std::sqrt(T * (1 + 1e-4));
+    double e = 2.0 * s->max_e, ref = (ix->d + 2) * std::ldexp(1.0, -24) * 1.01;
+    return (s->gamma_acc * 2.01 * 2 * s->max_n + 2 * s->max_r + e * (2 * sT + 3 * e) + ref * (sT + e) * (sT + e)) * 1.01;
+}
+
+hj_status tc_prepare(hj_index* ix, int kind, cudaStream_t st) {
+    if (ix->tc_kind == kind && ix->tc_state) return HJ_OK;
+    const uint32_t kpad = kpad_for(ix->d), n = ix->n, d = ix->d;
+    dfree(ix->tc_a, st);
+    dfree(ix->tc_b, st);
+    dfree(ix->tc_err, st);
+    uint16_t *qf = nullptr, *cf = nullptr;
+    float* origin = nullptr;
+    float4* pinfo = nullptr;
+    HJ_TRY(dalloc(&qf, (size_t)n * kpad, st));
+    HJ_TRY(dalloc(&cf, (size_t)n * kpad, st));
+    HJ_TRY(dalloc(&pinfo, n, st));
+    HJ_TRY(dalloc(&origin, d, st));
+    k_col_min<<<d, 256, 0, st>>>((const float*)ix->pts, n, d, origin);
+    HJ_LAUNCHED();
+    if (kind == HJ_REFINE_TC_BF16)
+        k_tc_prep<__nv_bfloat16><<<(n + 255) / 256, 256, 0, st>>>((const float*)ix->pts, n, d, kpad, origin,
+                                                                   (__nv_bfloat16*)qf, (__nv_bfloat16*)cf, pinfo);
+    else
+        k_tc_prep<__half><<<(n + 255) / 256, 256, 0, st>>>((const float*)ix->pts, n, d, kpad, origin, (__half*)qf,
+                                                            (__half*)cf, pinfo);
+    HJ_LAUNCHED();
+    dfree(origin, st);
+    ix->tc_a = qf;
+    ix->tc_b = cf;
+    ix->tc_err = reinterpret_cast<float*>(pinfo);
+    ix->tc_kpad = kpad;
+    ix->tc_kind = kind;
+    if (!ix->tc_state) ix->tc_state = new TcState();
+    TcState* s = tc_state(ix);
+    HJ_TRY(make_map(&s->maps.query, qf, n, kpad, kind));
+    HJ_TRY(make_map(&s->maps.cand, cf, n, kpad, kind));
+    // Accumulation model: each K=16 MMA step adds 16 exact products to the FP32
+    // accumulator with at most 2 ulps of the largest magnitude per term lost
+    // (alignment and truncation); bound = (steps + 1) * 32 * 2^-23 * sum|terms|.
+    s->gamma_acc = (float)((kpad / 16 + 1) * 32 * std::ldexp(1.0, -23));
+    // global maxima of the per-point terms, for the reported delta
+    std::vector<float4> hp(n);
+    HJ_CUDA(cudaMemcpyAsync(hp.data(), pinfo, (size_t)n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    HJ_CUDA(cudaStreamSynchronize(st));
+    s->max_e = s->max_n = s->max_r = 0;
+    for (const float4& p : hp) {
+        s->max_e = std::max(s->max_e, p.x);
+        s->max_n = std::max(s->max_n, p.y);
+        s->max_r = std::max(s->max_r, p.z);
+    }
+    return HJ_OK;
+}
+
+void tc_release(hj_index* ix) {
+    delete tc_state(ix);
+    ix->tc_state = nullptr;
+}
+
+hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t nblocks, unsigned int* head,
+                           const PairSink& sink, const PairSink& band, uint32_t count_only,
+                           unsigned long long* block_counts, unsigned long long* stats, uint32_t* err,
+                           cudaStream_t st) {
+    if (nblocks == 0) return HJ_OK;
+    TcState* s = tc_state(ix);
+    if (!s) { set_error("tensor-core operands not prepared"); return HJ_ERR_INVALID; }
+    const uint32_t nkb = ix->tc_kpad / 32, stages = tc_stages(nkb);
+    size_t smem = tc_smem_bytes(nkb, stages);
+    // one CTA per SM: ask for more than half of the SM's shared memory
+    smem = std::max<size_t>(smem, 116 * 1024);
+    static size_t configured = 0;
+    if (smem > configured) {
+        HJ_CUDA(cudaFuncSetAttribute(k_refine_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = smem;
+    }
+    TcArgs a{};
+    a.blocks = blocks; a.nblocks = nblocks; a.head = head;
+    a.perm = ix->perm; a.cell_lid = ix->cell_lid; a.cell_start = ix->cell_start; a.nC = ix->nC; a.grid = ix->grid;
+    a.pinfo = reinterpret_cast<const float4*>(ix->tc_err);
+    a.n = ix->n; a.nkb = nkb; a.stages = stages;
+    a.thr = (float)ix->thr;
+    a.gamma_acc = s->gamma_acc;
+    a.s_t = (float)(std::sqrt(ix->thr * (1 + 1e-4)) * (1 + 1e-6));
+    a.ref_rel = (float)((ix->d + 2) * std::ldexp(1.0, -24) * 1.01);
+    a.sink = sink; a.band = band;
+    a.count_only = count_only; a.block_counts = block_counts; a.stats = stats; a.err = err;
+    a.idesc = tc::idesc_f16(ix->tc_kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kTileRows);
+    unsigned grid = (unsigned)std::min<uint32_t>((uint32_t)num_sms(), nblocks);
+    k_refine_tc<<<grid, kThreads, smem, st>>>(s->maps.cand, s->maps.query, a);
+    HJ_LAUNCHED();
+    return HJ_OK;
+}
+
+hj_status launch_band_recheck(const hj_index* ix, const uint32_t* bq, const uint32_t* bc,
+                              const unsigned long long* band_used, unsigned long long band_cap, const PairSink& sink,
+                              cudaStream_t st) {
+    unsigned grid = (unsigned)num_sms() * 8;
+    k_band_recheck<<<grid, 256, 0, st>>>((const float*)ix->pts, ix->perm, ix->d, (float)ix->thr, bq, bc, band_used,
+                                         band_cap, sink);
+    HJ_LAUNCHED();
+    return HJ_OK;
+}
+
 }  // namespace hj
+
+extern "C" hj_status hj_probe_tc_tile(hj_index* ix, int kind, uint32_t a0, uint32_t b0, float* d_out,
+                                      void* h_query_rows, void* h_cand_rows, void* stream) {
+    using namespace hj;
+    if (!ix || !d_out || !tc_supported(ix, kind)) { set_error("hj_probe_tc_tile: unsupported"); return HJ_ERR_INVALID; }
+    cudaStream_t st = as_stream(stream);
+    HJ_TRY(tc_prepare(ix, kind, st));
+    TcState* s = tc_state(ix);
+    const uint32_t nkb = ix->tc_kpad / 32;
+    size_t smem = 1024 + (size_t)(kQT + 1) * nkb * kKBlockBytes + 64;
+    smem = std::max<size_t>(smem, 116 * 1024);
+    HJ_CUDA(cudaFuncSetAttribute(k_tc_tile_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    uint32_t* err = nullptr;
+    HJ_TRY(dalloc(&err, 1, st));
+    HJ_CUDA(cudaMemsetAsync(err, 0, 4, st));
+    k_tc_tile_probe<<<1, kThreads, smem, st>>>(s->maps.cand, s->maps.query, nkb,
+                                               tc::idesc_f16(kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kTileRows),
+                                               a0, b0, d_out, err);
+    HJ_LAUNCHED();
+    uint32_t herr = 0;
+    HJ_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
+    if (h_query_rows)
+        HJ_CUDA(cudaMemcpyAsync(h_query_rows, (const uint16_t*)ix->tc_a + (size_t)b0 * ix->tc_kpad,
+                                (size_t)std::min<uint32_t>(kQB, ix->n - b0) * ix->tc_kpad * 2, cudaMemcpyDeviceToHost, st));
+    if (h_cand_rows)
+        HJ_CUDA(cudaMemcpyAsync(h_cand_rows, (const uint16_t*)ix->tc_b + (size_t)a0 * ix->tc_kpad,
+                                (size_t)std::min<uint32_t>(kTileRows, ix->n - a0) * ix->tc_kpad * 2,
+                                cudaMemcpyDeviceToHost, st));
+    HJ_CUDA(cudaStreamSynchronize(st));
+    dfree(err, st);
+    if (herr) { set_error("hj_probe_tc_tile: a bounded wait expired"); return HJ_ERR_TIMEOUT; }
+    return HJ_OK;
+}

@@ -127,31 +127,69 @@ WORKLOADS = {
 }
 
 
-def mean_neighbours_sample(x: np.ndarray, eps: float, sample_frac: float = 0.01, seed: int = 12345,
-                           device: str = "cuda") -> float:
-    """Mean plain Euclidean neighbour count (self included) of a seeded query sample."""
-    import torch
-    n = x.shape[0]
+def _sample_queries(n: int, sample_frac: float, seed: int) -> np.ndarray:
     m = max(1, int(n * sample_frac))
     rng = np.random.default_rng(seed)
-    qi = np.sort(rng.choice(n, size=m, replace=False))
+    return np.sort(rng.choice(n, size=m, replace=False))
+
+
+def _d2_histogram(x: np.ndarray, qi: np.ndarray, edges, device: str) -> np.ndarray:
+    """Counts of (sampled query, point) squared distances per bin of `edges`."""
+    import torch
     X = torch.from_numpy(x).to(device=device, dtype=torch.float32)
     Q = X[torch.from_numpy(qi).to(device)]
-    tot = 0
-    for s in range(0, m, 1024):
-        d2 = torch.cdist(Q[s:s + 1024], X).square_()
-        tot += int((d2 <= eps * eps).sum().item())
-    return tot / m
+    E = torch.as_tensor(edges, dtype=torch.float32, device=device)
+    hist = torch.zeros(len(edges) + 1, dtype=torch.int64, device=device)
+    xn = (X * X).sum(1)
+    chunk = max(1, int(2e8 // x.shape[0]))
+    for s in range(0, len(qi), chunk):
+        q = Q[s:s + chunk]
+        d2 = (q * q).sum(1)[:, None] + xn[None, :] - 2.0 * (q @ X.T)
+        d2.clamp_(min=0)
+        hist += torch.bincount(torch.bucketize(d2.reshape(-1), E), minlength=len(edges) + 1)
+    return hist.cpu().numpy()
 
 
 def calibrate_eps(x: np.ndarray, target: float, sample_frac: float = 0.01, seed: int = 12345,
-                  device: str = "cuda", iters: int = 40) -> float:
-    """Bisect epsilon so the sampled mean neighbour count reaches `target`."""
-    lo, hi = 0.0, 1.0
-    for _ in range(iters):
-        mid = 0.5 * (lo + hi)
-        if mean_neighbours_sample(x, mid, sample_frac, seed, device) < target:
-            lo = mid
-        else:
-            hi = mid
-    return float(np.float32(hi))
+                  device: str = "cuda") -> float:
+    """Epsilon whose mean neighbour count (self included) over a seeded 1% query
+    sample, counted against the full dataset, first reaches `target`.
+
+    Two histogram passes on the GPU: log-spaced bins over d2, then linear bins
+    inside the bin where the mean crosses the target.  Returned as the dataset's
+    float32 value.
+    """
+    qi = _sample_queries(x.shape[0], sample_frac, seed)
+    m = len(qi)
+    edges = np.geomspace(1e-10, 4.0 * x.shape[1], 4000)
+    h = _d2_histogram(x, qi, edges, device)
+    cum = np.cumsum(h)[:-1] / m            # mean count with d2 <= edges[i]
+    i = int(np.searchsorted(cum, target))
+    lo = edges[i - 1] if i > 0 else 0.0
+    hi = edges[min(i, len(edges) - 1)]
+    fine = np.linspace(lo, hi, 2001)
+    h2 = _d2_histogram(x, qi, fine, device)
+    base = cum[i - 1] if i > 0 else 0.0
+    cum2 = base + np.cumsum(h2)[:-1] / m - (np.sum(h2[:1]) / m if i > 0 else 0.0)
+    j = min(int(np.searchsorted(cum2, target)), len(fine) - 1)
+    return float(np.float32(np.sqrt(fine[j])))
+
+
+def mean_neighbours_sample(x: np.ndarray, eps: float, sample_frac: float = 0.01, seed: int = 12345,
+                           device: str = "cuda") -> float:
+    qi = _sample_queries(x.shape[0], sample_frac, seed)
+    h = _d2_histogram(x, qi, np.array([eps * eps]), device)
+    return float(h[0]) / len(qi)
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+    out = {}
+    for name in sys.argv[1:]:
+        w = WORKLOADS[name]
+        x = w.generate()
+        e = calibrate_eps(x, w.target_neighbours)
+        out[name] = {"eps": e, "eps_repr": repr(e), "mean_neighbours": mean_neighbours_sample(x, e),
+                     "target": w.target_neighbours}
+        print(json.dumps({name: out[name]}), flush=True)

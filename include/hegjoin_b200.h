@@ -99,6 +99,8 @@ typedef struct {
     uint32_t max_batches;          /* safety cap on batch count; 0 = unlimited */
     uint32_t use_graphs;           /* replay the per-batch sequence through a CUDA graph */
     uint32_t keep_keys;            /* keep per-batch sorted key arrays (needed for the reference export) */
+    uint32_t shard_count;          /* multi-GPU: work items i with i % shard_count == shard_index (0 = all) */
+    uint32_t shard_index;
 } hj_join_opts;
 
 typedef struct {
@@ -110,6 +112,8 @@ typedef struct {
     uint64_t estimated_pairs;      /* selectivity estimate before the join */
     double filter_delta;           /* guard band half-width on d2 (tensor-core filter) */
     float ms_estimate, ms_refine, ms_group, ms_total;
+    float ms_refine_kernel;        /* device time of the refine kernels (CUDA events on the join's stream) */
+    uint32_t refine_launches;      /* refine kernel launches timed in ms_refine_kernel */
     uint32_t refine_used;          /* HJ_REFINE_* actually used */
     uint32_t kernel_launches;      /* kernels launched by this join */
 } hj_join_stats;
@@ -196,6 +200,15 @@ hj_status hj_self_join_host(const void* h_db, uint32_t n, uint32_t d, uint32_t k
  * d2 per pair.  Used to establish the FMA contraction the reference gets. */
 hj_status hj_probe_sqdist(const void* d_a, const void* d_b, uint32_t n, uint32_t d, int dtype,
                           void* d_out, void* stream);
+
+/* Evaluates one candidate tile (128 rows from sorted position a0) against 512
+ * query rows (from sorted position b0) through the tensor-core filter's TMA
+ * and tcgen05 path, writing the 128 x 512 FP32 accumulators (row = candidate,
+ * column = query) to d_out.  Optionally copies the quantised operand rows
+ * (query form 512 x kpad and candidate form 128 x kpad, 16-bit, kpad =
+ * 32 * ceil((d + 4) / 32)) to host buffers.  Synchronises `stream`. */
+hj_status hj_probe_tc_tile(hj_index* ix, int refine_kind, uint32_t a0, uint32_t b0, float* d_out,
+                           void* h_query_rows, void* h_cand_rows, void* stream);
 
 #ifdef __cplusplus
 }

@@ -36,8 +36,12 @@ def _load():
         getattr(lib, f"hjo_cell_workload_{suf}").restype = U64
         getattr(lib, f"hjo_join_{suf}").argtypes = [P, U32, U32, U32, T, P, P, I, P, P, P]
         getattr(lib, f"hjo_join_{suf}").restype = U64
+        getattr(lib, f"hjo_join_sample_{suf}").argtypes = [P, U32, U32, U32, T, P, P, P, U32, P]
+        getattr(lib, f"hjo_join_sample_{suf}").restype = U64
         getattr(lib, f"hjo_sqdist_{suf}").argtypes = [P, P, U32, I]
         getattr(lib, f"hjo_sqdist_{suf}").restype = D
+    lib.hjo_ref_cell_order.argtypes = [P, U32, P]
+    lib.hjo_ref_cell_order.restype = None
     lib.hjo_digest.argtypes = [P, P, U32, P, P]
     lib.hjo_digest.restype = None
     lib.hjo_num_threads.restype = I
@@ -119,6 +123,21 @@ def join(db: np.ndarray, k: int, eps, min_arr=None, n_cells=None, fma_mode: int 
     return off, vals[:total]
 
 
+def join_sample(db: np.ndarray, k: int, eps, qids: np.ndarray, min_arr=None, n_cells=None):
+    """Pairs emitted by the sampled queries and the seconds the refine took (all OpenMP threads)."""
+    db = np.ascontiguousarray(db)
+    n, d = db.shape
+    if min_arr is None or n_cells is None:
+        min_arr, _, n_cells, _ = geometry(db, k, eps)
+    mn = np.ascontiguousarray(min_arr, dtype=db.dtype)
+    nc = np.ascontiguousarray(n_cells, dtype=np.uint32)
+    q = np.ascontiguousarray(qids, dtype=np.uint32)
+    sec = ctypes.c_double()
+    pairs = getattr(lib, f"hjo_join_sample_{_suf(db)}")(_p(db), n, d, k, db.dtype.type(eps), _p(mn), _p(nc), _p(q),
+                                                       len(q), ctypes.byref(sec))
+    return int(pairs), float(sec.value)
+
+
 def digest(off: np.ndarray, vals: np.ndarray):
     """Per-query (count, sum of mix64(id), xor of mix64(id ^ salt))."""
     n = len(off) - 1
@@ -150,6 +169,51 @@ def sq_threshold(eps, dtype) -> float:
         else:
             break
     return x
+
+
+def ref_cell_order(nb: np.ndarray) -> np.ndarray:
+    """The reference's std::sort order of cells by candidate count (SortByWorkload.cu:97-98)."""
+    nb = np.ascontiguousarray(nb, dtype=np.uint32)
+    out = np.zeros(len(nb), np.int32)
+    lib.hjo_ref_cell_order(_p(nb), len(nb), _p(out))
+    return out
+
+
+def ref_batches(counts: np.ndarray, origin: np.ndarray):
+    """The reference's batch plan (GPUBatchEst_v2, GPU.cu:403-779) from exact per-query counts.
+
+    `counts` is indexed by original query id, `origin` is originPointIndex.
+    Returns (GPUBufferSize, [(first, second)], actual pairs per batch); the
+    estimate's unfilled tail is taken as zero.
+    """
+    n = len(origin)
+    n_est = int(n * 0.10)
+    r = counts[origin[np.arange(n_est) * 10]].astype(np.int64)
+    seqs = n // 10
+    full = np.zeros(n, np.int64)
+    full_est = 0
+    for i in range(seqs - 1):
+        m = max(r[i], r[i + 1])
+        full[i * 10] = r[i]
+        full[i * 10 + 1:(i + 1) * 10] = m
+        full_est += r[i] + 9 * m
+    buf = 50_000_000
+    if full_est < buf * 6:
+        buf = full_est // 6
+    reserve = int(buf * 0.05)
+    batches = []
+    b0, run = 0, 0
+    for i in range(n):
+        run += int(full[i])
+        if buf - reserve <= run:
+            batches.append((b0, i))
+            b0, run = i, 0
+        elif i == n - 1:
+            batches.append((b0, n))
+    per_q = counts[origin].astype(np.int64)
+    csum = np.concatenate([[0], np.cumsum(per_q)])
+    actual = [int(csum[b] - csum[a]) for a, b in batches]
+    return buf, batches, actual
 
 
 def num_threads() -> int:

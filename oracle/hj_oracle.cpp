@@ -252,6 +252,34 @@ HJO_WORK(double, f64)
 HJO_JOIN(float, f32)
 HJO_JOIN(double, f64)
 
+// The join restricted to a sample of query ids (the timed CPU baseline):
+// returns the number of pairs the sampled queries emit.
+#define HJO_JOIN_SAMPLE(T, SUF)                                                                      \
+    uint64_t hjo_join_sample_##SUF(const T* db, uint32_t n, uint32_t d, uint32_t k, T eps,            \
+                                   const T* minArr, const uint32_t* nCells, const uint32_t* qids,    \
+                                   uint32_t nq, double* seconds) {                                    \
+        Index ix;                                                                                    \
+        build_index<T>(db, n, d, k, eps, minArr, nCells, ix);                                        \
+        double t0 = omp_get_wtime();                                                                 \
+        uint64_t total = 0;                                                                          \
+        _Pragma("omp parallel for schedule(dynamic, 1) reduction(+ : total)")                        \
+        for (int64_t s = 0; s < (int64_t)nq; ++s) {                                                  \
+            const T* p = db + (size_t)qids[s] * d;                                                   \
+            uint64_t cnt = 0;                                                                        \
+            for_each_stencil_cell<T>(p, k, eps, minArr, nCells, ix, [&](int64_t ci) {                \
+                for (int32_t j = ix.first[ci]; j <= ix.last[ci]; ++j) {                              \
+                    T acc = sqdist<T>(db + (size_t)ix.lookup[j] * d, p, d, 1);                       \
+                    cnt += std::sqrt(acc) <= eps;                                                    \
+                }                                                                                    \
+            });                                                                                      \
+            total += cnt;                                                                            \
+        }                                                                                            \
+        *seconds = omp_get_wtime() - t0;                                                             \
+        return total;                                                                                \
+    }
+HJO_JOIN_SAMPLE(float, f32)
+HJO_JOIN_SAMPLE(double, f64)
+
 // Squared distance of one pair in the reference order (for error statistics).
 double hjo_sqdist_f32(const float* a, const float* b, uint32_t d, int fma_mode) {
     return (double)sqdist<float>(a, b, d, fma_mode);
@@ -275,6 +303,21 @@ void hjo_digest(const uint64_t* offsets, const uint32_t* vals, uint32_t n, uint6
         sum_out[q] = s;
         xor_out[q] = x;
     }
+}
+
+// SortByWorkload.cu:97-98 orders the schedulingCell array (in cell order,
+// cellId = cell index) with std::sort on nbPoints descending.  Replaying that
+// exact call on the same input gives the reference's (implementation-defined)
+// order among equal counts, which its batch estimator then depends on.
+struct HjoSchedCell {
+    int nbPoints;
+    int cellId;
+};
+void hjo_ref_cell_order(const uint32_t* nbPoints, uint32_t ncells, int32_t* order_out) {
+    std::vector<HjoSchedCell> v(ncells);
+    for (uint32_t i = 0; i < ncells; ++i) v[i] = HjoSchedCell{(int)nbPoints[i], (int)i};
+    std::sort(v.begin(), v.end(), [](const HjoSchedCell& a, const HjoSchedCell& b) { return a.nbPoints > b.nbPoints; });
+    for (uint32_t i = 0; i < ncells; ++i) order_out[i] = v[i].cellId;
 }
 
 int hjo_num_threads(void) { return omp_get_max_threads(); }
