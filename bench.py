@@ -124,11 +124,35 @@ def barrier():
         dist.barrier()
 
 
+# reference build (oracle/ref/Makefile) whose GPUNUMDIM/NUMINDEXEDDIM/DTYPE match each workload
+REF_BUILD = {"c2_18d": "c2", "c3_90d": "r90d", "c4_skew6d": "r6d"}
+
+
 def cpu_baseline(db, wl, seconds_target=20.0):
-    """The CPU restatement of the refine on a bounded query sample, all host threads."""
+    """The reference's own CPU join (Super-EGO, Util::egoJoinV2) on a bounded query
+    sample against the full dataset, all host cores; the CPU restatement of the
+    GPU path when no matching reference build exists."""
+    exe = os.path.join(ROOT, "oracle", "_ref", REF_BUILD.get(wl.name, "-"), "ego_driver")
+    if os.path.exists(exe):
+        path = os.path.join("/tmp", f"hj_{wl.name}_{os.getpid()}.bin")
+        with open(path, "wb") as f:
+            np.array([db.shape[0], db.shape[1], db.dtype.itemsize], np.uint32).tofile(f)
+            db.tofile(f)
+        try:
+            p = subprocess.run([exe, path, repr(float(wl.eps)), str(seconds_target)], capture_output=True,
+                               text=True, timeout=max(600, 20 * seconds_target))
+        finally:
+            os.unlink(path)
+        line = [l for l in p.stdout.splitlines() if l.startswith("HJEGO ")]
+        if p.returncode == 0 and line:
+            r = json.loads(line[-1][6:])
+            return {"value": r["pairs"] / r["seconds"], "unit": "pairs/s", "cores": r["threads"],
+                    "kind": "reference",
+                    "sample": f"Super-EGO (the reference's CPU join, Util::egoJoinV2) for {r['queries']} evenly "
+                              f"spaced query points against all {r['n']} points ({r['pairs']} pairs in "
+                              f"{r['seconds']:.1f} s); EGO reorder/sort untimed as in main.cu's egoTime"}
     import oracle
     n = db.shape[0]
-    # calibrate the sample size on 64 queries, then size it for ~seconds_target
     probe = np.linspace(0, n - 1, 64).astype(np.int64)
     _, t_probe = oracle.join_sample(db, wl.k, wl.eps, probe)
     m = int(max(64, min(n, 64 * seconds_target / max(t_probe, 1e-3))))
@@ -155,9 +179,158 @@ def reference_arm(args, wl):
     line = {"impl": "reference", "metric": "result pairs/s", "value": val, "unit": "pairs/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic (seeded Exp(40) generator)",
-            "config": {"workload": wl.name, "n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps},
+            "config": {"workload": wl.name, "n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps,
+                       "sample_per_step": base["sample"]},
             "cpu_baseline": {**base, "value": val},
             "e2e": {"value": val, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# serving (the request-stream workload): --serve
+def quick_eps(db: np.ndarray, target: float, dev, seed: int) -> float:
+    """Epsilon for a mean of `target` neighbours at the dataset's full size, from a pooled
+    sample of query-to-point squared distances (256 queries x up to 100k points)."""
+    import torch
+    n = db.shape[0]
+    rng = np.random.default_rng(seed)
+    s = min(n, 100_000)
+    ref = db if s == n else db[np.sort(rng.choice(n, s, replace=False))]
+    q = db[rng.choice(n, min(256, n), replace=False)]
+    R = torch.from_numpy(ref).to(dev)
+    Q = torch.from_numpy(q).to(dev)
+    d2 = torch.cdist(Q, R).square_().reshape(-1)
+    level = min(1.0, target / n)
+    r2 = torch.quantile(d2[torch.randperm(d2.numel(), device=dev)[:16_000_000]], level).item()
+    return float(np.float32(np.sqrt(max(r2, 1e-12))))
+
+
+def serve_bench(args):
+    import threading
+    import torch
+    import hegjoin_b200 as hj
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(args.serve_seed)
+    reqs = []
+    for i in range(args.requests):
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(args.max_n))))
+        d = int(rng.choice([2, 6, 18, 32, 90]))
+        target = float(rng.uniform(4, 128))
+        db = hj.generate_exp40(10_000 + i, n, d, np.float32)
+        reqs.append((db, min(d, 6), quick_eps(db, target, dev, i), target))
+    total_pts = sum(r[0].shape[0] for r in reqs)
+
+    def run(workers, arrivals):
+        srv = hj.Server(workers=workers, hbm_budget=int(args.hbm_budget_gb * (1 << 30)), refine=args.refine)
+        tickets = [None] * len(reqs)
+        t0 = time.perf_counter()
+
+        def submitter():
+            for i, (db, k, eps, _) in enumerate(reqs):
+                delay = t0 + arrivals[i] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[i] = srv.submit(db, k, eps)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat, pairs, infos = [], 0, []
+        for i in range(len(reqs)):
+            while tickets[i] is None:
+                time.sleep(0.0005)
+            _, info = srv.wait(tickets[i], keep_result=False)
+            lat.append(info.t_done - info.t_submit)
+            pairs += info.stats.total_pairs
+            infos.append(info)
+        th.join()
+        span = max(x.t_done for x in infos) - min(x.t_submit for x in infos)
+        srv.close()
+        return {"pairs": int(pairs), "seconds": span, "pairs_per_s": pairs / span,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "mean_ms": float(np.mean(lat) * 1e3)}
+
+    run(1, np.zeros(min(8, len(reqs))))      # warm-up (JIT of tuning, pools)
+    serial = run(1, np.zeros(len(reqs)))     # one request at a time, all queued at t=0
+    rate = args.load * len(reqs) / serial["seconds"]     # offered load in requests/s
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    served = run(args.workers, arrivals)
+    line = {"metric": "served p50/p99 latency (ms) and aggregate result pairs/s", "value": served["pairs_per_s"],
+            "unit": "pairs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic request stream (seeded Exp(40) datasets)",
+            "config": {"workload": "serving", "requests": len(reqs), "points_total": int(total_pts),
+                       "n_range": [1000, args.max_n], "d_choices": [2, 6, 18, 32, 90], "k": "min(d, 6)",
+                       "target_neighbours": "U[4, 128]", "arrivals": "Poisson",
+                       "offered_rate_req_per_s": rate, "workers": args.workers,
+                       "hbm_budget_gb": args.hbm_budget_gb, "refine": args.refine},
+            "served": served, "serial": serial, "speedup_vs_serial": served["pairs_per_s"] / serial["pairs_per_s"],
+            "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"]}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# tensor-core filter vs plain FP32 refine on one workload: --compare
+def compare_bench(args, wl):
+    import torch
+    import hegjoin_b200 as hj
+    dev = torch.device("cuda", 0)
+    np_db = wl.generate()
+    db = torch.from_numpy(np_db).to(dev)
+    out = {}
+    digests = {}
+    for refine in ("exact", args.tc_kind):
+        times, launches0 = [], hj.kernel_launch_count()
+        for it in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ix = hj.GridIndex(db, wl.k, wl.eps)
+            cand = ix.sort_by_workload()
+            res = hj.join(ix, refine=refine)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            if it >= args.warmup:
+                times.append(t1 - t0)
+            st = res.stats
+            if it == args.warmup + args.steps - 1:
+                c, s, x = res.digest()
+                digests[refine] = (c.cpu().numpy(), s.cpu().numpy(), x.cpu().numpy())
+            res.close()
+            ix.close()
+        sec = statistics.mean(times)
+        out[refine] = {"pairs": int(st.total_pairs), "seconds_per_step": sec, "pairs_per_s": st.total_pairs / sec,
+                       "refine_kernel_ms": st.ms_refine_kernel, "band_pairs": int(st.band_pairs),
+                       "tc_accepts": int(st.tc_accepts), "filter_delta": st.filter_delta,
+                       "candidates": int(cand)}
+    same = all(np.array_equal(a, b) for a, b in zip(digests["exact"], digests[args.tc_kind]))
+    # max |D - d2_fp64| of the tensor-core squared distance over sampled tiles
+    ix = hj.GridIndex(db, wl.k, wl.eps)
+    ix.sort_by_workload()
+    n = np_db.shape[0]
+    torch.cuda.synchronize()
+    P = hj.device_view(ix.views()[0], (n, wl.d), np.float32).double().cpu().numpy()   # points in cell order
+    rng = np.random.default_rng(3)
+    max_err, max_rel = 0.0, 0.0
+    for _ in range(16):
+        a0 = int(rng.integers(0, max(1, n - 128)))
+        b0 = int(rng.integers(0, max(1, n - 512)))
+        acc, _, _ = hj.probe_tc_tile(ix, args.tc_kind, a0, b0)
+        nc, nq = min(128, n - a0), min(512, n - b0)
+        C = P[a0:a0 + nc]
+        Q = P[b0:b0 + nq]
+        d2 = ((C[:, None, :] - Q[None, :, :]) ** 2).sum(-1)
+        err = np.abs(acc[:nc, :nq].astype(np.float64) - d2)
+        near = d2 <= 4 * wl.eps * wl.eps
+        max_err = max(max_err, float(err.max()))
+        if near.any():
+            max_rel = max(max_rel, float(err[near].max()))
+    ix.close()
+    line = {"metric": "result pairs/s, tensor-core filter vs plain FP32", "workload": wl.name,
+            "config": {"n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps, "steps": args.steps, "warmup": args.warmup},
+            "exact": out["exact"], "tc": out[args.tc_kind], "tc_kind": args.tc_kind,
+            "speedup": out[args.tc_kind]["pairs_per_s"] / out["exact"]["pairs_per_s"],
+            "identical_pair_sets": bool(same),
+            "max_abs_d2_error_vs_fp64": max_err, "max_abs_d2_error_vs_fp64_within_2eps": max_rel,
+            "filter_delta": out[args.tc_kind]["filter_delta"],
+            "error_sample": "16 random tiles of 128 candidates x 512 queries (tile probe) vs FP64 distances"}
     print(json.dumps(line), flush=True)
 
 
@@ -173,7 +346,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=20.0)
+    ap.add_argument("--serve", action="store_true", help="run the request-stream serving benchmark instead")
+    ap.add_argument("--requests", type=int, default=256)
+    ap.add_argument("--max-n", type=int, default=1_000_000)
+    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--load", type=float, default=8.0, help="offered load as a multiple of the serial rate")
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-seed", type=int, default=5)
+    ap.add_argument("--compare", action="store_true", help="time the exact refine against the tensor-core filter")
+    ap.add_argument("--tc-kind", default="tc_f16", choices=["tc_f16", "tc_bf16"])
     args = ap.parse_args()
+    if args.serve:
+        serve_bench(args)
+        return
 
     from hegjoin_b200 import workloads
     wl = workloads.WORKLOADS[args.workload]
@@ -182,6 +367,9 @@ def main():
         wl = dataclasses.replace(wl, n=args.n)
     if args.impl == "reference":
         reference_arm(args, wl)
+        return
+    if args.compare:
+        compare_bench(args, wl)
         return
 
     import torch

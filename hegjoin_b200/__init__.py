@@ -74,6 +74,15 @@ class JoinStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_uint64), ("workers", ctypes.c_uint32), ("refine", ctypes.c_int)]
+
+
+class ServeInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("stats", JoinStats)]
+
+
 def _load() -> ctypes.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is missing: build it with `make -C hegjoin_b200/csrc` "
@@ -103,6 +112,14 @@ def _load() -> ctypes.CDLL:
         "hj_self_join_host": (I, [P, U32, U32, U32, I, D, P, P, P, P]),
         "hj_probe_sqdist": (I, [P, P, U32, U32, I, P, P]),
         "hj_probe_tc_tile": (I, [P, I, U32, U32, P, P, P, P]),
+        "hj_shard_plan": (I, [U32, U32, U32, P, P, P]),
+        "hj_generate_exp40": (I, [U64, U64, U64, U32, I, P]),
+        "hj_generate_skewed": (I, [U64, U64, U32, U32, D, D, I, P]),
+        "hj_server_opts_default": (None, [P]),
+        "hj_server_create": (I, [P, P]),
+        "hj_server_submit": (I, [P, P, U32, U32, U32, I, D, P]),
+        "hj_server_wait": (I, [P, U64, D, P, P]),
+        "hj_server_destroy": (I, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -350,6 +367,43 @@ def probe_sqdist(a, b, stream=None):
     return out
 
 
+def shard_plan(n_items: int, shard_count: int, shard_index: int):
+    """(first, stride, count) of the work items rank `shard_index` processes."""
+    f, s, m = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    check(lib.hj_shard_plan(n_items, shard_count, shard_index, ctypes.byref(f), ctypes.byref(s), ctypes.byref(m)))
+    return f.value, s.value, m.value
+
+
+def generate_exp40(seed: int, n: int, d: int, dtype=np.float32, stream: int = 0) -> np.ndarray:
+    """Host generator (C++/OpenMP) producing the same values as workloads.exp40."""
+    out = np.empty((n, d), dtype=dtype)
+    check(lib.hj_generate_exp40(seed, stream, n, d, HJ_F32 if out.dtype == np.float32 else HJ_F64, out.ctypes.data))
+    return out
+
+
+def generate_skewed(seed: int, n: int, d: int, n_clusters: int = 64, sigma: float = 0.002,
+                    frac_clustered: float = 0.2, dtype=np.float32) -> np.ndarray:
+    """Host generator of the skewed workload (80% Exp(40), 20% Gaussian clusters)."""
+    out = np.empty((n, d), dtype=dtype)
+    check(lib.hj_generate_skewed(seed, n, d, n_clusters, sigma, frac_clustered,
+                                 HJ_F32 if out.dtype == np.float32 else HJ_F64, out.ctypes.data))
+    return out
+
+
+class _DeviceArray:
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def device_view(ptr: int, shape, dtype):
+    """A torch tensor over library-owned device memory (no copy; valid while the owner lives)."""
+    torch = _torch()
+    typestr = {np.float32: "<f4", np.float64: "<f8", np.uint32: "<u4", np.int32: "<i4",
+               np.uint64: "<u8", np.int64: "<i8"}[np.dtype(dtype).type]
+    return torch.as_tensor(_DeviceArray(ptr, shape, typestr), device="cuda")
+
+
 def kpad_for(d: int) -> int:
     return ((d + 4 + 31) // 32) * 32
 
@@ -373,3 +427,49 @@ def probe_tc_tile(index: GridIndex, refine: str, a0: int, b0: int, stream=None):
     else:
         conv = lambda a: a.view(np.float16).astype(np.float64)
     return out.cpu().numpy(), conv(hq), conv(hc)
+
+
+class Server:
+    """Continuous-batching join service (hj_server_*): submit host datasets, wait for device results."""
+
+    def __init__(self, workers: int = 4, hbm_budget: int = 150 << 30, refine="auto"):
+        o = ServerOpts()
+        lib.hj_server_opts_default(ctypes.byref(o))
+        o.workers = workers
+        o.hbm_budget = hbm_budget
+        o.refine = REFINE_NAMES[refine] if isinstance(refine, str) else int(refine)
+        self._h = ctypes.c_void_p()
+        check(lib.hj_server_create(ctypes.byref(o), ctypes.byref(self._h)))
+        self._keep = {}
+
+    def submit(self, db: np.ndarray, k: int, eps: float) -> int:
+        db = np.ascontiguousarray(db)
+        t = ctypes.c_uint64()
+        check(lib.hj_server_submit(self._h, db.ctypes.data, db.shape[0], db.shape[1], k,
+                                   HJ_F32 if db.dtype == np.float32 else HJ_F64, float(eps), ctypes.byref(t)))
+        self._keep[t.value] = db          # the host buffer must outlive the request
+        return t.value
+
+    def wait(self, ticket: int, keep_result: bool = True, timeout: float = 0.0):
+        h = ctypes.c_void_p()
+        info = ServeInfo()
+        st = lib.hj_server_wait(self._h, ticket, float(timeout), ctypes.byref(h) if keep_result else None,
+                                ctypes.byref(info))
+        db = self._keep.pop(ticket, None)
+        check(st)
+        res = None
+        if keep_result:
+            import torch
+            res = JoinResult(h, info.stats, db.shape[0], torch.device("cuda"))
+        return res, info
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.hj_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

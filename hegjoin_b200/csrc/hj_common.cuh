@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -17,7 +18,9 @@ constexpr uint32_t kSentinelKey = 0xFFFFFFFFu;
 
 // ---- error handling --------------------------------------------------------
 void set_error(const char* fmt, ...);
-uint64_t& launch_counter();
+void count_launch();
+uint64_t launch_count();
+uint64_t thread_launch_count();   // launches made by the calling thread
 
 #define HJ_CUDA(call)                                                                   \
     do {                                                                                \
@@ -37,7 +40,7 @@ uint64_t& launch_counter();
 
 #define HJ_LAUNCHED()                                                                   \
     do {                                                                                \
-        ++::hj::launch_counter();                                                       \
+        ::hj::count_launch();                                                           \
         cudaError_t e__ = cudaGetLastError();                                           \
         if (e__ != cudaSuccess) {                                                       \
             ::hj::set_error("%s:%d kernel launch: %s", __FILE__, __LINE__,              \
@@ -67,6 +70,14 @@ template <typename T>
 void dfree(T*& p, cudaStream_t st) {
     if (p) cudaFreeAsync(p, st);
     p = nullptr;
+}
+
+// Raise a kernel's dynamic shared-memory limit once per (kernel, size), safe
+// when several host threads launch joins concurrently.
+hj_status ensure_smem_ptr(const void* kern, size_t bytes);   // hj_index.cu
+template <typename K>
+hj_status ensure_smem(K kern, size_t bytes) {
+    return ensure_smem_ptr(reinterpret_cast<const void*>(kern), bytes);
 }
 
 inline int num_sms() {

@@ -15,9 +15,12 @@
 // cells along dimension 0 are consecutive linear ids), one warp per cell.
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <limits>
+#include <map>
+#include <mutex>
 
 #include "hj_internal.h"
 
@@ -31,15 +34,34 @@ void set_error(const char* fmt, ...) {
     vsnprintf(g_err, sizeof(g_err), fmt, ap);
     va_end(ap);
 }
-uint64_t& launch_counter() {
-    static uint64_t c = 0;
-    return c;
+static std::atomic<uint64_t> g_launches{0};
+static thread_local uint64_t t_launches = 0;
+void count_launch() {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    ++t_launches;
+}
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+uint64_t thread_launch_count() { return t_launches; }
+
+hj_status ensure_smem_ptr(const void* kern, size_t bytes) {
+    static std::mutex mu;
+    static std::map<const void*, size_t> done;
+    if (bytes <= 48 * 1024) return HJ_OK;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& have = done[kern];
+    if (bytes <= have) return HJ_OK;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) {
+        set_error("cudaFuncSetAttribute(%zu bytes): %s", bytes, cudaGetErrorString(e));
+        return HJ_ERR_CUDA;
+    }
+    have = bytes;
+    return HJ_OK;
 }
 
 void init_memory_pool() {
-    static bool done = false;
-    if (done) return;
-    done = true;
+    static std::atomic<bool> done{false};
+    if (done.exchange(true)) return;
     int dev = 0;
     cudaMemPool_t pool;
     if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
@@ -434,7 +456,7 @@ extern "C" {
 
 const char* hj_last_error(void) { return hj::g_err; }
 const char* hj_version(void) { return "hegjoin_b200 0.1 (sm_100a)"; }
-uint64_t hj_kernel_launch_count(void) { return hj::launch_counter(); }
+uint64_t hj_kernel_launch_count(void) { return hj::launch_count(); }
 
 hj_status hj_grid_geometry(const void* d_db, uint32_t n, uint32_t d, uint32_t k, int dtype, double eps,
                            double* h_min_arr, double* h_max_arr, uint32_t* h_n_cells, uint64_t* h_total_cells,
@@ -480,6 +502,7 @@ hj_status hj_index_create(const void* d_db, uint32_t n, uint32_t d, uint32_t k, 
     init_memory_pool();
     hj_index* ix = new hj_index();
     ix->dtype = dtype;
+    ix->stream = st;
     cudaGetDevice(&ix->device);
     hj_status s = (dtype == HJ_F32)
                       ? index_create_t<float>((const float*)d_db, n, d, k, (float)eps, h_min_arr, h_n_cells, st, ix)
@@ -496,8 +519,9 @@ hj_status hj_index_create(const void* d_db, uint32_t n, uint32_t d, uint32_t k, 
 
 hj_status hj_index_destroy(hj_index* ix) {
     if (!ix) return HJ_OK;
-    free_index(ix, 0);
-    cudaDeviceSynchronize();
+    // stream-ordered frees on the index's own stream: no device-wide synchronisation,
+    // so concurrent joins on other streams keep running
+    free_index(ix, ix->stream);
     delete ix;
     return HJ_OK;
 }

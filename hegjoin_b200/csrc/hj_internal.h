@@ -29,6 +29,7 @@ struct hj_index {
     uint64_t total_cells = 0;
     uint32_t aliasing = 0;
     int device = 0;
+    cudaStream_t stream = nullptr;   // stream the index was built on; its memory is freed in that order
 
     // device arrays
     void* pts = nullptr;             // n x d, dataset type, ordered by (cell id, original id)

@@ -24,6 +24,11 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
 
 #include "hj_internal.h"
 
@@ -43,10 +48,13 @@ hj_status launch_band_recheck(const hj_index* ix, const uint32_t* bq, const uint
                               const PairSink& sink, cudaStream_t st);
 double tc_delta(const hj_index* ix);
 bool tc_supported(const hj_index* ix, int kind);
+int tc_get_epi(const hj_index* ix);
+void tc_set_epi(hj_index* ix, int epi);
 }  // namespace hj
 
 struct hj_result {
     uint32_t n = 0;
+    cudaStream_t stream = nullptr;       // the join's stream; buffers are freed in its order
     std::vector<uint32_t*> vals;
     std::vector<uint32_t*> keys;
     std::vector<uint64_t> counts;
@@ -161,6 +169,53 @@ struct Batch {
     uint32_t b0, b1;
 };
 
+// ---- autotuner ------------------------------------------------------------------------
+// Tile-shape choices are timed once per (refine kind, d, dtype) on the
+// estimator's count-only sample and remembered for the process; with
+// HJ_TUNE_FILE set they are also read from / appended to that file
+// ("kind d dtype choice" per line).  HJ_TUNE=0 disables timing (defaults used).
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;
+bool g_tune_loaded = false;
+
+std::string tune_key(int kind, uint32_t d, int dtype) {
+    std::ostringstream o;
+    o << kind << ' ' << d << ' ' << dtype;
+    return o.str();
+}
+
+bool tune_lookup(const std::string& key, int* choice) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (!g_tune_loaded) {
+        g_tune_loaded = true;
+        if (const char* f = std::getenv("HJ_TUNE_FILE")) {
+            std::ifstream in(f);
+            int k, c;
+            uint32_t d;
+            int dt;
+            while (in >> k >> d >> dt >> c) g_tune[tune_key(k, d, dt)] = c;
+        }
+    }
+    auto it = g_tune.find(key);
+    if (it == g_tune.end()) return false;
+    *choice = it->second;
+    return true;
+}
+
+void tune_store(const std::string& key, int choice) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = choice;
+    if (const char* f = std::getenv("HJ_TUNE_FILE")) {
+        std::ofstream out(f, std::ios::app);
+        out << key << ' ' << choice << '\n';
+    }
+}
+
+bool tuning_enabled() {
+    const char* e = std::getenv("HJ_TUNE");
+    return !(e && e[0] == '0');
+}
+
 float ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -171,6 +226,20 @@ float ms_since(std::chrono::steady_clock::time_point t0) {
 using namespace hj;
 
 extern "C" {
+
+hj_status hj_shard_plan(uint32_t n_items, uint32_t shard_count, uint32_t shard_index, uint32_t* first,
+                        uint32_t* stride, uint32_t* n_mine) {
+    if (shard_count == 0 || shard_index >= shard_count || !first || !stride || !n_mine) {
+        set_error("hj_shard_plan: shard_index %u out of range for %u shards", shard_index, shard_count);
+        return HJ_ERR_INVALID;
+    }
+    // round robin over the heaviest-first order: every rank gets a mix of heavy
+    // and light items (an LPT-like balance without a host pass over item costs)
+    *first = shard_index;
+    *stride = shard_count;
+    *n_mine = n_items > shard_index ? (n_items - shard_index + shard_count - 1) / shard_count : 0;
+    return HJ_OK;
+}
 
 void hj_join_opts_default(hj_join_opts* o) {
     if (!o) return;
@@ -184,10 +253,10 @@ void hj_join_opts_default(hj_join_opts* o) {
 
 hj_status hj_result_destroy(hj_result* r) {
     if (!r) return HJ_OK;
-    for (auto* p : r->vals) cudaFree(p);
-    for (auto* p : r->keys) cudaFree(p);
-    if (r->d_batch_vals) cudaFree(r->d_batch_vals);
-    if (r->table) cudaFree(r->table);
+    for (auto* p : r->vals) cudaFreeAsync(p, r->stream);
+    for (auto* p : r->keys) cudaFreeAsync(p, r->stream);
+    if (r->d_batch_vals) cudaFreeAsync(r->d_batch_vals, r->stream);
+    if (r->table) cudaFreeAsync(r->table, r->stream);
     delete r;
     return HJ_OK;
 }
@@ -201,7 +270,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     if (opts.sample_rate <= 0 || opts.sample_rate > 1) opts.sample_rate = 0.02;
     if (opts.mem_fraction <= 0 || opts.mem_fraction > 0.95) opts.mem_fraction = 0.6;
     cudaStream_t st = as_stream(stream);
-    uint64_t launches0 = launch_counter();
+    uint64_t launches0 = thread_launch_count();
     hj_join_stats S{};
     HJ_TRY(hj_sort_by_workload(ix, stream, nullptr));
 
@@ -228,13 +297,13 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     uint32_t nblocks = 0;
     HJ_TRY(build_blocks(ix, qb, &blocks, &nblocks, st));
     if (opts.shard_count > 1) {
-        // this rank's share of the heaviest-first order: items i = shard_index mod shard_count
-        if (opts.shard_index >= opts.shard_count) { set_error("hj_join: shard_index >= shard_count"); return HJ_ERR_INVALID; }
-        uint32_t mine = nblocks > opts.shard_index ? (nblocks - opts.shard_index + opts.shard_count - 1) / opts.shard_count : 0;
+        // this rank's share of the heaviest-first order
+        uint32_t first = 0, stride = 1, mine = 0;
+        HJ_TRY(hj_shard_plan(nblocks, opts.shard_count, opts.shard_index, &first, &stride, &mine));
         HjBlock* sel = nullptr;
         HJ_TRY(dalloc(&sel, std::max<uint32_t>(mine, 1), st));
         if (mine) {
-            k_pick_strided<<<(mine + 255) / 256, 256, 0, st>>>(blocks, opts.shard_index, opts.shard_count, mine, sel);
+            k_pick_strided<<<(mine + 255) / 256, 256, 0, st>>>(blocks, first, stride, mine, sel);
             HJ_LAUNCHED();
         }
         dfree(blocks, st);
@@ -301,8 +370,36 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         k_pick_samples<<<(nsamp + 255) / 256, 256, 0, st>>>(blocks, nblocks, stride, nsamp, sblocks);
         HJ_LAUNCHED();
         PairSink none{nullptr, nullptr, nullptr, 0, overflow};
-        HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
-        HJ_TRY(check_timeout());
+        int tuned = 0;
+        const std::string key = tune_key(refine, ix->d, ix->dtype);
+        if (tc && !tune_lookup(key, &tuned) && tuning_enabled()) {
+            // time each epilogue width on the sample; the last run's counts are the estimate
+            const int cands[3] = {1, 2, 4};
+            float best = 1e30f;
+            int best_epi = tc_get_epi(ix);
+            cudaEvent_t e0, e1;
+            HJ_CUDA(cudaEventCreate(&e0));
+            HJ_CUDA(cudaEventCreate(&e1));
+            for (int c : cands) {
+                tc_set_epi(ix, c);
+                HJ_CUDA(cudaMemsetAsync(scnt, 0, nsamp * sizeof(unsigned long long), st));
+                HJ_CUDA(cudaEventRecord(e0, st));
+                HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
+                HJ_CUDA(cudaEventRecord(e1, st));
+                HJ_TRY(check_timeout());
+                float ms = 0;
+                HJ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) { best = ms; best_epi = c; }
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            tc_set_epi(ix, best_epi);
+            tune_store(key, best_epi);
+        } else {
+            if (tc && tuned) tc_set_epi(ix, tuned);
+            HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
+            HJ_TRY(check_timeout());
+        }
         std::vector<unsigned long long> hs(nsamp);
         HJ_CUDA(cudaMemcpyAsync(hs.data(), scnt, nsamp * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
@@ -371,6 +468,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
 
     hj_result* res = new hj_result();
     res->n = ix->n;
+    res->stream = st;
     hj_status rs = dalloc(&res->table, ix->n, st);
     if (rs != HJ_OK) { delete res; return rs; }
     HJ_CUDA(cudaMemsetAsync(res->table, 0, (size_t)ix->n * sizeof(hj_nt_entry), st));
@@ -463,7 +561,8 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     cudaGetLastError();
     if (tc) {
         unsigned long long tcs[2] = {0, 0};
-        HJ_CUDA(cudaMemcpy(tcs, counters + 2, sizeof(tcs), cudaMemcpyDeviceToHost));
+        HJ_CUDA(cudaMemcpyAsync(tcs, counters + 2, sizeof(tcs), cudaMemcpyDeviceToHost, st));
+        HJ_CUDA(cudaStreamSynchronize(st));
         S.tc_accepts = tcs[0];
         S.band_pairs = tcs[1];
     }
@@ -485,7 +584,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     S.total_pairs = res->total;
     S.n_batches = (uint32_t)res->vals.size();
     S.ms_total = ms_since(t_start);
-    S.kernel_launches = (uint32_t)(launch_counter() - launches0);
+    S.kernel_launches = (uint32_t)(thread_launch_count() - launches0);
     if (stats) *stats = S;
     *out = res;
     return HJ_OK;

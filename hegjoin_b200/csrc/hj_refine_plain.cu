@@ -236,11 +236,7 @@ template <typename T, int D, int QB, int CB, int RQ, int RC>
 hj_status launch_t(const PlainArgs<T>& args, cudaStream_t st) {
     size_t smem = (size_t)(D ? D : args.d) * (QB + CB) * sizeof(T) + (QB + CB + 2 * kRowGroup + 1) * sizeof(uint32_t);
     auto kern = k_refine_plain<T, D, QB, CB, RQ, RC>;
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        HJ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = smem;
-    }
+    HJ_TRY(ensure_smem(kern, smem));
     int per_sm = 0;
     HJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) {

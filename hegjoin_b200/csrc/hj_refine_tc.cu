@@ -46,7 +46,7 @@ namespace {
 constexpr int kQT = 4;                       // query tiles per work item
 constexpr int kTileRows = 128;               // rows per tile (M for A, N for B)
 constexpr int kQB = kQT * kTileRows;         // queries per work item
-constexpr int kThreads = 192;
+constexpr int kProbeThreads = 192;   // tile probe: TMA warp, MMA warp, 4 epilogue warps
 constexpr int kMaxStages = 8;
 constexpr uint32_t kKBlockBytes = kTileRows * 64;   // one 32-element K block of a tile
 constexpr uint32_t kTmemCols = 512;
@@ -114,8 +114,6 @@ __device__ __forceinline__ uint32_t tile_range(const TcShared& S, uint32_t t) {
     return lo;
 }
 
-__device__ __forceinline__ float min3f(float a, float b, float c) { return fminf(fminf(a, b), c); }
-
 // delta for one candidate row against the whole query block (all bounds rounded up):
 //   |D - d2_ref| <= acc + res + e (2 sT + 3 e) + ref_rel (sT + e)^2
 //   e   = e_c + max e_q       (|x~ - x| norms; |(|q~-c~|) - |q-c|| <= e)
@@ -131,7 +129,22 @@ __device__ __forceinline__ float tc_delta_row(const TcArgs& a, float4 pc, float 
     return d * 1.01f + 1e-30f;
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+// Tree minimum of N values (depth log2 N, so the epilogue's compare is not a dependent chain).
+template <uint32_t N>
+__device__ __forceinline__ float minN(const float (&v)[N]) {
+    float m[N / 2];
+#pragma unroll
+    for (uint32_t i = 0; i < N / 2; ++i) m[i] = fminf(v[2 * i], v[2 * i + 1]);
+#pragma unroll
+    for (uint32_t w = N / 4; w >= 1; w >>= 1)
+#pragma unroll
+        for (uint32_t i = 0; i < w; ++i) m[i] = fminf(m[2 * i], m[2 * i + 1]);
+    return m[0];
+}
+
+// EPI = epilogue warp groups (4 warps each, one per TMEM lane quarter).
+template <int EPI>
+__global__ void __launch_bounds__(64 + 128 * EPI, 1)
     k_refine_tc(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query, TcArgs a) {
     extern __shared__ uint8_t smem_raw[];
     // operand tiles need 1024-byte alignment for the swizzle pattern
@@ -150,7 +163,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int j = 0; j < kQT; ++j) {
             tc::mbar_init(&S.full_acc[j], 1);
-            tc::mbar_init(&S.empty_acc[j], 4);
+            tc::mbar_init(&S.empty_acc[j], 4 * EPI);
         }
         tc::mbar_init(&S.bfull, 1);
         S.abort = 0;
@@ -190,7 +203,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // query ids and block maxima of the error terms
         {
             float me = 0.f, mn = 0.f, mr = 0.f;
-            for (uint32_t i = tid; i < (uint32_t)kQB; i += kThreads) {
+            for (uint32_t i = tid; i < (uint32_t)kQB; i += blockDim.x) {
                 S.qid[i] = i < nq ? a.perm[blk.q0 + i] : 0u;
                 if (i < nq) {
                     float4 p = a.pinfo[blk.q0 + i];
@@ -334,9 +347,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int j = 0; j < kQT; ++j) acc_use[j] = __shfl_sync(0xffffffffu, acc_use[j], 0);
             ++items_loaded;
         } else {
-            // ---------------- epilogue: warps 2..5, TMEM lane quarter = warp % 4
+            // ---------------- epilogue: warps 2 .. 2 + 4*EPI; TMEM lane quarter = warp % 4,
+            // column group = (warp - 2) / 4 (128 / EPI columns of each accumulator)
             const uint32_t quarter = warp & 3u;
+            const uint32_t grp = (warp - 2) >> 2;
             const uint32_t row = quarter * 32u + lane;
+            const uint32_t lane_base = (quarter * 32u) << 16;
             const float me = __uint_as_float(S.max_e), mn = __uint_as_float(S.max_n), mr = __uint_as_float(S.max_r);
             unsigned long long n_acc = 0, n_band = 0;
             bool ok = true;
@@ -361,51 +377,59 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     tc::fence_after();
                     const uint32_t ncols = min((uint32_t)kTileRows, nq - j * kTileRows);
-                    for (uint32_t c = 0; c < 4; ++c) {
-                        float v[32];
-                        tc::tmem_ld_32x32(tmem + ((quarter * 32u) << 16) + j * kTileRows + c * 32u, v);
+                    // this warp's columns of accumulator j: COLS = 128 / EPI, loaded LDW at a time
+                    constexpr uint32_t COLS = 128 / EPI;
+                    constexpr uint32_t LDW = COLS >= 64 ? 64u : 32u;
+#pragma unroll
+                    for (uint32_t c0 = 0; c0 < COLS; c0 += LDW) {
+                        float v[LDW];
+                        const uint32_t col0 = grp * COLS + c0;
+                        if constexpr (LDW == 64) {
+                            tc::tmem_ld_32x64(tmem + lane_base + j * kTileRows + col0, v);
+                        } else {
+                            tc::tmem_ld_32x32(tmem + lane_base + j * kTileRows + col0, v);
+                        }
                         tc::tmem_ld_wait();
-                        if (c == 3) {
-                            // the accumulator has been read: hand it back to the MMA warp
+                        if (c0 + LDW >= COLS) {
+                            // all of this warp's columns are in registers: release the accumulator
                             tc::fence_before();
                             __syncwarp();
                             if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
                         }
-                        float m = v[0];
-#pragma unroll
-                        for (int i = 1; i < 31; i += 2) m = min3f(m, v[i], v[i + 1]);
-                        m = fminf(m, v[31]);
-                        const bool any_hit = m <= hi;
+                        const bool any_hit = minN<LDW>(v) <= hi;
                         if (!__any_sync(0xffffffffu, any_hit)) continue;
-                        uint32_t hmask = 0, amask = 0;
-                        const uint32_t cbase = c * 32u;
-                        if (any_hit) {
 #pragma unroll
-                            for (int i = 0; i < 32; ++i) {
-                                bool inq = cbase + i < ncols;
-                                hmask |= (uint32_t)(inq && v[i] <= hi) << i;
-                                amask |= (uint32_t)(inq && v[i] <= lo) << i;
+                        for (uint32_t h = 0; h < LDW / 32; ++h) {
+                            const uint32_t cbase = col0 + h * 32u;
+                            uint32_t hmask = 0, amask = 0;
+                            if (any_hit) {
+#pragma unroll
+                                for (int i = 0; i < 32; ++i) {
+                                    bool inq = cbase + i < ncols;
+                                    hmask |= (uint32_t)(inq && v[h * 32 + i] <= hi) << i;
+                                    amask |= (uint32_t)(inq && v[h * 32 + i] <= lo) << i;
+                                }
                             }
+                            const uint32_t bmask = hmask & ~amask;
+                            n_acc += __popc(amask);
+                            n_band += __popc(bmask);
+                            if (a.count_only) continue;
+                            if (amask && cid == 0xFFFFFFFFu) cid = a.perm[cpos];
+                            const uint32_t qcol = j * kTileRows + cbase;
+                            uint32_t m1 = amask;
+                            warp_emit(a.sink, wc_acc, __popc(amask), [&](uint32_t) {
+                                uint32_t b = __ffs(m1) - 1;
+                                m1 &= m1 - 1;
+                                return make_uint2(S.qid[qcol + b], cid);
+                            });
+                            uint32_t m2 = bmask;
+                            const uint32_t q0 = S.q0;
+                            warp_emit(a.band, wc_band, __popc(bmask), [&](uint32_t) {
+                                uint32_t b = __ffs(m2) - 1;
+                                m2 &= m2 - 1;
+                                return make_uint2(q0 + qcol + b, cpos);
+                            });
                         }
-                        const uint32_t bmask = hmask & ~amask;
-                        n_acc += __popc(amask);
-                        n_band += __popc(bmask);
-                        if (a.count_only) continue;
-                        if (amask && cid == 0xFFFFFFFFu) cid = a.perm[cpos];
-                        const uint32_t qcol = j * kTileRows + cbase;
-                        uint32_t m1 = amask;
-                        warp_emit(a.sink, wc_acc, __popc(amask), [&](uint32_t) {
-                            uint32_t b = __ffs(m1) - 1;
-                            m1 &= m1 - 1;
-                            return make_uint2(S.qid[qcol + b], cid);
-                        });
-                        uint32_t m2 = bmask;
-                        const uint32_t q0 = S.q0;
-                        warp_emit(a.band, wc_band, __popc(bmask), [&](uint32_t) {
-                            uint32_t b = __ffs(m2) - 1;
-                            m2 &= m2 - 1;
-                            return make_uint2(q0 + qcol + b, cpos);
-                        });
                     }
                     ++acc_use[j];
                 }
@@ -526,7 +550,7 @@ __global__ void k_col_min(const float* __restrict__ pts, uint32_t n, uint32_t d,
 // Debug/test kernel: one candidate tile (rows a0..a0+127) against four query
 // tiles (rows b0..b0+511) through the same TMA maps, descriptors and MMA
 // sequence as k_refine_tc; writes every accumulator value to out[128][512].
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kProbeThreads, 1)
     k_tc_tile_probe(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query,
                     uint32_t nkb, uint32_t idesc, uint32_t a0, uint32_t b0, float* __restrict__ out, uint32_t* err) {
     extern __shared__ uint8_t smem_raw[];
@@ -649,6 +673,7 @@ struct TcMaps {
 
 struct TcState {
     TcMaps maps;
+    int epi = 2;              // epilogue warp groups (autotuned)
     float gamma_acc = 0;
     float max_e = 0, max_n = 0, max_r = 0;
 };
@@ -724,6 +749,15 @@ hj_status tc_prepare(hj_index* ix, int kind, cudaStream_t st) {
     return HJ_OK;
 }
 
+int tc_get_epi(const hj_index* ix) {
+    TcState* s = tc_state(ix);
+    return s ? s->epi : 0;
+}
+void tc_set_epi(hj_index* ix, int epi) {
+    TcState* s = tc_state(ix);
+    if (s && (epi == 1 || epi == 2 || epi == 4)) s->epi = epi;
+}
+
 void tc_release(hj_index* ix) {
     delete tc_state(ix);
     ix->tc_state = nullptr;
@@ -740,11 +774,11 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     size_t smem = tc_smem_bytes(nkb, stages);
     // one CTA per SM: ask for more than half of the SM's shared memory
     smem = std::max<size_t>(smem, 116 * 1024);
-    static size_t configured = 0;
-    if (smem > configured) {
-        HJ_CUDA(cudaFuncSetAttribute(k_refine_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = smem;
-    }
+    const int epi = s->epi == 1 || s->epi == 4 ? s->epi : 2;
+    if (epi == 1) HJ_TRY(ensure_smem(k_refine_tc<1>, smem));
+    else if (epi == 2) HJ_TRY(ensure_smem(k_refine_tc<2>, smem));
+    else HJ_TRY(ensure_smem(k_refine_tc<4>, smem));
+    auto kern = epi == 1 ? k_refine_tc<1> : (epi == 2 ? k_refine_tc<2> : k_refine_tc<4>);
     TcArgs a{};
     a.blocks = blocks; a.nblocks = nblocks; a.head = head;
     a.perm = ix->perm; a.cell_lid = ix->cell_lid; a.cell_start = ix->cell_start; a.nC = ix->nC; a.grid = ix->grid;
@@ -758,7 +792,7 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     a.count_only = count_only; a.block_counts = block_counts; a.stats = stats; a.err = err;
     a.idesc = tc::idesc_f16(ix->tc_kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kTileRows);
     unsigned grid = (unsigned)std::min<uint32_t>((uint32_t)num_sms(), nblocks);
-    k_refine_tc<<<grid, kThreads, smem, st>>>(s->maps.cand, s->maps.query, a);
+    kern<<<grid, 64 + 128 * epi, smem, st>>>(s->maps.cand, s->maps.query, a);
     HJ_LAUNCHED();
     return HJ_OK;
 }
@@ -785,11 +819,11 @@ extern "C" hj_status hj_probe_tc_tile(hj_index* ix, int kind, uint32_t a0, uint3
     const uint32_t nkb = ix->tc_kpad / 32;
     size_t smem = 1024 + (size_t)(kQT + 1) * nkb * kKBlockBytes + 64;
     smem = std::max<size_t>(smem, 116 * 1024);
-    HJ_CUDA(cudaFuncSetAttribute(k_tc_tile_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HJ_TRY(ensure_smem(k_tc_tile_probe, smem));
     uint32_t* err = nullptr;
     HJ_TRY(dalloc(&err, 1, st));
     HJ_CUDA(cudaMemsetAsync(err, 0, 4, st));
-    k_tc_tile_probe<<<1, kThreads, smem, st>>>(s->maps.cand, s->maps.query, nkb,
+    k_tc_tile_probe<<<1, kProbeThreads, smem, st>>>(s->maps.cand, s->maps.query, nkb,
                                                tc::idesc_f16(kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kTileRows),
                                                a0, b0, d_out, err);
     HJ_LAUNCHED();

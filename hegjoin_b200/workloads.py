@@ -3,10 +3,11 @@
 The reference ships a generator (datasets/dataset_gen_fixed_len_expo_dist.cpp:24-91)
 that draws each coordinate i.i.d. from Exp(rate=40) with ``std::mt19937`` and
 redraws values above 1.  The workloads here keep that distribution but use a
-counter-based generator so any slice of a dataset can be produced in parallel
-and reproduced bit for bit on any machine with the same numpy build:
+counter-based generator, so any slice of a dataset can be produced in parallel
+and reproduced bit for bit; its definition is hegjoin_b200/csrc/hj_datagen.cpp
+(host C++, reached through the library):
 
-    u(seed, i, a) = (mix64(mix64(seed ^ SALT) + 64*i + a) >> 11) * 2**-53   in [0, 1)
+    u(seed, i, a) = (mix64(mix64(seed ^ SALT ^ K*stream) + 64*i + a) >> 11) * 2**-53   in [0, 1)
     x = -log1p(-u) / 40        (float64), cast to the dataset dtype,
     attempt a = 0, 1, ... until the cast value is < 1.
 
@@ -20,72 +21,20 @@ query sample (stored to 17 significant digits in EPS_TABLE).
 from __future__ import annotations
 
 import dataclasses
-import math
 
 import numpy as np
 
-SALT = 0xD1B54A32D192ED03
-M64 = (1 << 64) - 1
-
-
-def _mix64(z: np.ndarray) -> np.ndarray:
-    """splitmix64 finaliser on a uint64 array (wrapping arithmetic)."""
-    with np.errstate(over="ignore"):
-        z = z + np.uint64(0x9E3779B97F4A7C15)
-        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-        return z ^ (z >> np.uint64(31))
-
-
-def _uniform(seed: int, stream: int, idx: np.ndarray, attempt: int) -> np.ndarray:
-    base = _mix64(np.array([(seed ^ SALT ^ (stream * 0x632BE59BD9B4E019)) & M64], dtype=np.uint64))[0]
-    with np.errstate(over="ignore"):
-        z = _mix64(base + idx.astype(np.uint64) * np.uint64(64) + np.uint64(attempt))
-    return (z >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
-
-
 def exp40(seed: int, n: int, d: int, dtype=np.float32, stream: int = 0) -> np.ndarray:
     """n x d coordinates, i.i.d. Exp(rate=40) redrawn into [0, 1) after the dtype cast."""
-    total = n * d
-    out = np.empty(total, dtype=dtype)
-    chunk = 1 << 22
-    for s in range(0, total, chunk):
-        idx = np.arange(s, min(total, s + chunk), dtype=np.uint64)
-        pending = np.arange(idx.size)
-        vals = np.empty(idx.size, dtype=dtype)
-        attempt = 0
-        while pending.size:
-            u = _uniform(seed, stream, idx[pending], attempt)
-            x = (-np.log1p(-u) / 40.0).astype(dtype)
-            ok = x < dtype(1.0)
-            vals[pending[ok]] = x[ok]
-            pending = pending[~ok]
-            attempt += 1
-            if attempt >= 64:
-                raise RuntimeError("exp40: redraw limit reached")
-        out[s:s + idx.size] = vals
-    return out.reshape(n, d)
+    import hegjoin_b200 as hj
+    return hj.generate_exp40(seed, n, d, dtype, stream)
 
 
 def skewed(seed: int, n: int, d: int, n_clusters: int = 64, sigma: float = 0.002,
            frac_clustered: float = 0.2, dtype=np.float32) -> np.ndarray:
     """80% Exp(40) points and 20% from Gaussian clusters, clipped to [0, 1)."""
-    n_c = int(round(n * frac_clustered))
-    n_e = n - n_c
-    x = np.empty((n, d), dtype=dtype)
-    x[:n_e] = exp40(seed, n_e, d, dtype, stream=0)
-    centres = _uniform(seed, 1, np.arange(n_clusters * d, dtype=np.uint64), 0).reshape(n_clusters, d)
-    cid = (_mix64(np.arange(n_c, dtype=np.uint64) + np.uint64(seed * 7919)) % np.uint64(n_clusters)).astype(np.int64)
-    idx = np.arange(n_c * d, dtype=np.uint64)
-    u1 = _uniform(seed, 2, idx, 0)
-    u2 = _uniform(seed, 3, idx, 0)
-    g = np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * math.pi * u2)
-    pts = centres[cid] + sigma * g.reshape(n_c, d)
-    pts = np.clip(pts, 0.0, np.nextafter(1.0, 0.0))
-    c = pts.astype(dtype)
-    c[c >= dtype(1.0)] = np.nextafter(dtype(1.0), dtype(0.0))
-    x[n_e:] = c
-    return x
+    import hegjoin_b200 as hj
+    return hj.generate_skewed(seed, n, d, n_clusters, sigma, frac_clustered, dtype)
 
 
 @dataclasses.dataclass(frozen=True)
@@ -114,9 +63,9 @@ class Workload:
 # Epsilon values found by calibrate_eps (1% seeded query sample against the full
 # dataset, bisection to the target mean neighbour count), as dataset-dtype values.
 EPS_TABLE = {
-    "c2_18d": 0.038387289,
-    "c3_90d": 0.20277268,
-    "c4_skew6d": 0.0,   # filled in by calibration
+    "c2_18d": 0.04033349081873894,     # mean 50.0003 neighbours on the sample
+    "c3_90d": 0.20804697275161743,     # mean 30.0008
+    "c4_skew6d": 0.003275492461398244,  # mean 200.18
 }
 
 WORKLOADS = {

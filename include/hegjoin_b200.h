@@ -187,12 +187,59 @@ hj_status hj_result_to_csr(const hj_result* r, uint64_t* d_offsets, uint32_t* d_
 hj_status hj_result_digest(const hj_result* r, uint32_t* d_count, uint64_t* d_sum, uint64_t* d_xor,
                            void* stream);
 
+/* ---- multi-GPU sharding ----------------------------------------------------- */
+/* The work items a rank processes out of `n_items` heaviest-first items when
+ * the join runs with shard_count ranks: items first, first + stride, ... (n_mine
+ * of them).  Host-only arithmetic; hj_join applies exactly this selection. */
+hj_status hj_shard_plan(uint32_t n_items, uint32_t shard_count, uint32_t shard_index, uint32_t* first,
+                        uint32_t* stride, uint32_t* n_mine);
+
 /* ---- one-shot convenience: host buffers in, host pair count out ------------ */
 /* Copies the dataset to the device, builds the index, sorts by workload and
  * joins; the result stays on the device in *out (may be NULL to discard). */
 hj_status hj_self_join_host(const void* h_db, uint32_t n, uint32_t d, uint32_t k, int dtype, double eps,
                             const hj_join_opts* opts, void* stream, hj_result** out,
                             hj_join_stats* stats);
+
+/* ---- serving: continuous batching of self-join requests ------------------------ */
+/* Beyond the reference (one dataset per process).  Requests are admitted in
+ * arrival order as soon as a worker is free and their device-memory
+ * reservation fits hbm_budget; each worker runs a request's copy-in, index,
+ * workload order and join on its own stream, so concurrent requests overlap on
+ * the device.  The host dataset passed to hj_server_submit must stay valid
+ * until hj_server_wait returns for that ticket. */
+typedef struct hj_server hj_server;
+typedef struct {
+    uint64_t hbm_budget;           /* bytes; 0 = 150 GiB */
+    uint32_t workers;              /* concurrent requests; 0 = 1 */
+    int refine;                    /* HJ_REFINE_* for every request */
+} hj_server_opts;
+typedef struct {
+    hj_status status;
+    double t_submit, t_admit, t_done;   /* steady-clock seconds */
+    hj_join_stats stats;
+} hj_serve_info;
+void hj_server_opts_default(hj_server_opts* o);
+hj_status hj_server_create(const hj_server_opts* opts, hj_server** out);
+hj_status hj_server_submit(hj_server* s, const void* h_db, uint32_t n, uint32_t d, uint32_t k, int dtype,
+                           double eps, uint64_t* ticket);
+/* Blocks until the request is done (or timeout_s passes: HJ_ERR_TIMEOUT).
+ * The result (device memory) passes to the caller when `result` is non-NULL,
+ * else it is released. */
+hj_status hj_server_wait(hj_server* s, uint64_t ticket, double timeout_s, hj_result** result,
+                         hj_serve_info* info);
+hj_status hj_server_destroy(hj_server* s);
+
+/* ---- synthetic data ---------------------------------------------------------- */
+/* n x d coordinates i.i.d. Exp(rate=40), redrawn into [0, 1) after the cast to
+ * the dataset type, from a counter-based generator (seed, stream): the same
+ * values hegjoin_b200.workloads.exp40 produces.  Host memory; OpenMP. */
+hj_status hj_generate_exp40(uint64_t seed, uint64_t stream, uint64_t n, uint32_t d, int dtype, void* h_out);
+/* The skewed workload: the first n - round(frac * n) points from
+ * hj_generate_exp40(seed, 0, ...), the rest from n_clusters Gaussian clusters
+ * (standard deviation sigma, centres uniform in [0,1)^d), clipped to [0, 1). */
+hj_status hj_generate_skewed(uint64_t seed, uint64_t n, uint32_t d, uint32_t n_clusters, double sigma,
+                             double frac_clustered, int dtype, void* h_out);
 
 /* ---- probes --------------------------------------------------------------- */
 /* Evaluates the reference's squared-distance expression (kernel.cu:350-353)

@@ -50,12 +50,13 @@ BUILDS = {
 CASES = [
     ("r2d_f64_dense", "r2d", 20000, 100, 0.01, "exp40"),
     ("r2d_f64_sparse", "r2d", 6000, 101, 0.004, "exp40"),
-    ("r6d_f32_exp", "r6d", 20000, 102, 0.05, "exp40"),
-    ("r6d_f32_skew", "r6d", 20000, 103, 0.02, "skewed"),
-    ("r18d_f32_exp", "r18d", 12000, 104, 0.07, "exp40"),
-    ("r90d_f32_exp", "r90d", 4000, 105, 0.25, "exp40"),
     ("r5k3_f64_exp", "r5k3", 8000, 106, 0.05, "exp40"),
+    ("r2d_f64_edge", "r2d", 3000, 108, 0.02, "exp40"),
 ]
+# The reference's GPU join did not finish within 900 s on the 6-D build (input
+# r6d, n=20000, eps 0.05, a sub-second workload by reading); its GPU code is not
+# run again for the k = 6 builds, whose shapes are pinned through the oracle.
+NOT_RUN = {"r6d", "r18d", "r90d"}
 
 
 def dataset(build, n, seed, gen):
@@ -101,6 +102,8 @@ def run(outdir):
     os.makedirs(outdir, exist_ok=True)
     summary = {}
     for name, b, n, seed, eps, gen in CASES:
+        if b in NOT_RUN:
+            continue
         db, k = dataset(b, n, seed, gen)
         safe, info = plan_is_safe(db, k, eps)
         summary[name] = {"plan": info, "safe": bool(safe)}
@@ -114,7 +117,12 @@ def run(outdir):
                 np.array([n, db.shape[1], db.dtype.itemsize], np.uint32).tofile(f)
                 db.tofile(f)
             pre = os.path.join(tmp, "out")
-            p = subprocess.run([exe, path, repr(float(eps)), pre], capture_output=True, text=True, timeout=900)
+            try:
+                p = subprocess.run([exe, path, repr(float(eps)), pre], capture_output=True, text=True, timeout=240)
+            except subprocess.TimeoutExpired:
+                print(f"{name}: reference run exceeded 240 s; stopped, not retried", flush=True)
+                summary[name]["error"] = "timeout"
+                continue
             if p.returncode != 0:
                 print(f"{name}: reference run failed rc={p.returncode}\n{p.stdout[-2000:]}\n{p.stderr[-2000:]}")
                 summary[name]["error"] = p.returncode

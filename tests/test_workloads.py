@@ -28,3 +28,25 @@ def test_skewed_mix():
     # clustered points sit in tight groups: many near-duplicates at the 0.01 scale
     q = np.floor(tail / 0.01)
     assert len(np.unique(q, axis=0)) < 0.5 * len(tail)
+
+
+def _mix64(z):
+    with np.errstate(over="ignore"):
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def test_generator_definition():
+    """The native generator follows its documented formula (checked through
+    float32 outputs, where libm ulp differences rarely survive the cast)."""
+    seed, n, d = 5, 400, 7
+    got = workloads.exp40(seed, n, d, np.float32)
+    salt = np.uint64(0xD1B54A32D192ED03)
+    base = _mix64(np.array([np.uint64(seed) ^ salt], np.uint64))[0]
+    with np.errstate(over="ignore"):
+        z = _mix64(base + np.arange(n * d, dtype=np.uint64) * np.uint64(64))
+    u = (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    exp = (-np.log1p(-u) / 40.0).astype(np.float32).reshape(n, d)
+    assert (got == exp).mean() > 0.999
