@@ -220,13 +220,14 @@ def serve_bench(args):
         reqs.append((db, min(d, 6), quick_eps(db, target, dev, i), target))
     total_pts = sum(r[0].shape[0] for r in reqs)
 
-    def run(workers, arrivals):
+    def run(workers, arrivals, todo=None):
+        todo = reqs[:len(arrivals)] if todo is None else todo
         srv = hj.Server(workers=workers, hbm_budget=int(args.hbm_budget_gb * (1 << 30)), refine=args.refine)
-        tickets = [None] * len(reqs)
+        tickets = [None] * len(todo)
         t0 = time.perf_counter()
 
         def submitter():
-            for i, (db, k, eps, _) in enumerate(reqs):
+            for i, (db, k, eps, _) in enumerate(todo):
                 delay = t0 + arrivals[i] - time.perf_counter()
                 if delay > 0:
                     time.sleep(delay)
@@ -235,7 +236,7 @@ def serve_bench(args):
         th = threading.Thread(target=submitter)
         th.start()
         lat, pairs, infos = [], 0, []
-        for i in range(len(reqs)):
+        for i in range(len(todo)):
             while tickets[i] is None:
                 time.sleep(0.0005)
             _, info = srv.wait(tickets[i], keep_result=False)
@@ -249,7 +250,11 @@ def serve_bench(args):
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "mean_ms": float(np.mean(lat) * 1e3)}
 
-    run(1, np.zeros(min(8, len(reqs))))      # warm-up (JIT of tuning, pools)
+    # warm-up: one request of every dimension class (tile-shape tuning, memory pools)
+    first = {}
+    for r in reqs:
+        first.setdefault(r[0].shape[1], r)
+    run(1, np.zeros(len(first)), list(first.values()))
     serial = run(1, np.zeros(len(reqs)))     # one request at a time, all queued at t=0
     rate = args.load * len(reqs) / serial["seconds"]     # offered load in requests/s
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))

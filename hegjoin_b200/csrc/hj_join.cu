@@ -223,6 +223,15 @@ float ms_since(std::chrono::steady_clock::time_point t0) {
 }  // namespace
 }  // namespace hj
 
+namespace hj {
+// Re-associate a result with another stream for its frees.  The server calls
+// this with the legacy default stream once a worker has synchronised its own
+// stream, so results outlive the worker streams that produced them.
+void result_set_stream(hj_result* r, cudaStream_t s) {
+    if (r) r->stream = s;
+}
+}  // namespace hj
+
 using namespace hj;
 
 extern "C" {
@@ -427,7 +436,10 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     HJ_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const uint64_t chunk_slack = (uint64_t)num_sms() * 64 * kSinkChunk;   // partially filled warp chunks
     const double bytes_per_slot = 16.0 + 4.0 + (opts.keep_keys ? 4.0 : 0.0) + (tc ? 8.0 : 0.0);
-    uint64_t max_cap = (uint64_t)(opts.mem_fraction * (double)free_b / bytes_per_slot);
+    // leave room for the result itself (4 bytes per estimated pair, kept on the device)
+    const double result_bytes = 4.0 * total_est * (opts.keep_keys ? 2.0 : 1.0) * 1.1;
+    const double usable = std::max(0.0, (double)free_b - result_bytes);
+    uint64_t max_cap = (uint64_t)(opts.mem_fraction * usable / bytes_per_slot);
     max_cap = std::min<uint64_t>(max_cap, 0xF0000000ull);
     uint64_t want = (uint64_t)(total_est * 2.0) + chunk_slack + 4096;
     uint64_t cap = opts.result_capacity ? opts.result_capacity + chunk_slack : std::min(want, max_cap);

@@ -20,6 +20,8 @@
 // each thread evaluates an RQ x RC register tile of (query, candidate) pairs.
 // Hits are appended with warp-aggregated reservations into the pair sink.
 
+#include <type_traits>
+
 #include "hj_internal.h"
 
 namespace hj {
@@ -53,6 +55,22 @@ __device__ __forceinline__ uint32_t lower_bound_lid(const unsigned long long* a,
         if (a[mid] < v) lo = mid + 1; else hi = mid;
     }
     return lo;
+}
+
+// Packed FP32 pairs (sm_100): each lane's result is the IEEE-rounded scalar
+// operation, so the packed loop is bit-identical to the scalar one.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    return ((unsigned long long)__float_as_uint(hi) << 32) | __float_as_uint(lo);
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
 }
 
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
@@ -181,24 +199,58 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
                     const uint32_t nvalid = min((uint32_t)CB, total - cb);
 
                     T acc[RQ][RC];
-#pragma unroll
-                    for (int r = 0; r < RQ; ++r)
-#pragma unroll
-                        for (int c = 0; c < RC; ++c) acc[r][c] = T(0);
-#pragma unroll(D ? (D < 32 ? D : 8) : 1)
-                    for (uint32_t l = 0; l < d; ++l) {
-                        T qv[RQ], cv[RC];
-#pragma unroll
-                        for (int r = 0; r < RQ; ++r) qv[r] = q_s[l * QB + ty * RQ + r];
-#pragma unroll
-                        for (int c = 0; c < RC; ++c) cv[c] = c_s[l * CB + tx * RC + c];
+                    if constexpr (std::is_same<T, float>::value && RC % 2 == 0) {
+                        // candidate pairs (c, c+1) packed: diff = c - q, acc = fma(diff, diff, acc)
+                        unsigned long long acc2[RQ][RC / 2];
 #pragma unroll
                         for (int r = 0; r < RQ; ++r)
 #pragma unroll
-                            for (int c = 0; c < RC; ++c) {
-                                T diff = fsub(cv[c], qv[r]);          // candidate - query (kernel.cu:351)
-                                acc[r][c] = ffma(diff, diff, acc[r][c]);
+                            for (int c = 0; c < RC / 2; ++c) acc2[r][c] = 0ull;
+#pragma unroll(D ? (D <= 8 ? D : 6) : 1)
+                        for (uint32_t l = 0; l < d; ++l) {
+                            unsigned long long cv2[RC / 2];
+                            const unsigned long long* cp =
+                                reinterpret_cast<const unsigned long long*>(&c_s[l * CB + tx * RC]);
+#pragma unroll
+                            for (int c = 0; c < RC / 2; ++c) cv2[c] = cp[c];
+#pragma unroll
+                            for (int r = 0; r < RQ; ++r) {
+                                const float q = q_s[l * QB + ty * RQ + r];
+                                const unsigned long long qq = pack2(q, q);
+#pragma unroll
+                                for (int c = 0; c < RC / 2; ++c) {
+                                    unsigned long long diff = sub2(cv2[c], qq);   // candidate - query (kernel.cu:351)
+                                    acc2[r][c] = fma2(diff, diff, acc2[r][c]);
+                                }
                             }
+                        }
+#pragma unroll
+                        for (int r = 0; r < RQ; ++r)
+#pragma unroll
+                            for (int c = 0; c < RC / 2; ++c) {
+                                acc[r][2 * c] = __uint_as_float((uint32_t)acc2[r][c]);
+                                acc[r][2 * c + 1] = __uint_as_float((uint32_t)(acc2[r][c] >> 32));
+                            }
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < RQ; ++r)
+#pragma unroll
+                            for (int c = 0; c < RC; ++c) acc[r][c] = T(0);
+#pragma unroll(D ? (D <= 8 ? D : 6) : 1)
+                        for (uint32_t l = 0; l < d; ++l) {
+                            T qv[RQ], cv[RC];
+#pragma unroll
+                            for (int r = 0; r < RQ; ++r) qv[r] = q_s[l * QB + ty * RQ + r];
+#pragma unroll
+                            for (int c = 0; c < RC; ++c) cv[c] = c_s[l * CB + tx * RC + c];
+#pragma unroll
+                            for (int r = 0; r < RQ; ++r)
+#pragma unroll
+                                for (int c = 0; c < RC; ++c) {
+                                    T diff = fsub(cv[c], qv[r]);          // candidate - query (kernel.cu:351)
+                                    acc[r][c] = ffma(diff, diff, acc[r][c]);
+                                }
+                        }
                     }
                     uint32_t mask = 0;
 #pragma unroll

@@ -533,18 +533,28 @@ __global__ void k_tc_prep(const float* __restrict__ pts, uint32_t n, uint32_t d,
     pinfo[i] = make_float4((float)sqrt(e2) * up, (float)n2 * up, (float)res * up + 1e-30f, 0.f);
 }
 
+// Per-dimension minimum of the points: lanes walk a row's dimensions (coalesced
+// reads), warps stride over rows, one atomic per (block, dimension).
 __global__ void k_col_min(const float* __restrict__ pts, uint32_t n, uint32_t d, float* __restrict__ out) {
-    uint32_t l = blockIdx.x;
-    float m = INFINITY;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) m = fminf(m, pts[(size_t)i * d + l]);
-    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    __shared__ float w[32];
-    if (lane_id() == 0) w[threadIdx.x >> 5] = m;
+    extern __shared__ float part[];   // [warps][d]
+    const uint32_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
+    for (uint32_t l = lane_id(); l < d; l += 32) part[w * d + l] = INFINITY;
+    for (uint32_t i = blockIdx.x * warps + w; i < n; i += gridDim.x * warps)
+        for (uint32_t l = lane_id(); l < d; l += 32) part[w * d + l] = fminf(part[w * d + l], pts[(size_t)i * d + l]);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        for (uint32_t k = 1; k < blockDim.x / 32; ++k) m = fminf(m, w[k]);
-        out[l] = fminf(m, w[0]);
+    for (uint32_t l = threadIdx.x; l < d; l += blockDim.x) {
+        float m = INFINITY;
+        for (uint32_t k = 0; k < warps; ++k) m = fminf(m, part[k * d + l]);
+        // non-negative floats order like their bit patterns as ints; negative ones
+        // order in reverse as unsigned ints
+        if (m >= 0.f) atomicMin(reinterpret_cast<int*>(out) + l, __float_as_int(m));
+        else atomicMax(reinterpret_cast<unsigned int*>(out) + l, __float_as_uint(m));
     }
+}
+
+__global__ void k_fill_f32(float* p, uint32_t n, float v) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
 }
 
 // Debug/test kernel: one candidate tile (rows a0..a0+127) against four query
@@ -713,8 +723,13 @@ hj_status tc_prepare(hj_index* ix, int kind, cudaStream_t st) {
     HJ_TRY(dalloc(&cf, (size_t)n * kpad, st));
     HJ_TRY(dalloc(&pinfo, n, st));
     HJ_TRY(dalloc(&origin, d, st));
-    k_col_min<<<d, 256, 0, st>>>((const float*)ix->pts, n, d, origin);
+    k_fill_f32<<<(d + 255) / 256, 256, 0, st>>>(origin, d, INFINITY);
     HJ_LAUNCHED();
+    {
+        const unsigned blocks = (unsigned)std::min<uint32_t>(num_sms() * 2, std::max<uint32_t>(1, n / 64));
+        k_col_min<<<blocks, 256, (size_t)8 * d * sizeof(float), st>>>((const float*)ix->pts, n, d, origin);
+        HJ_LAUNCHED();
+    }
     if (kind == HJ_REFINE_TC_BF16)
         k_tc_prep<__nv_bfloat16><<<(n + 255) / 256, 256, 0, st>>>((const float*)ix->pts, n, d, kpad, origin,
                                                                    (__nv_bfloat16*)qf, (__nv_bfloat16*)cf, pinfo);

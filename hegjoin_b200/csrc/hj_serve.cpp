@@ -25,6 +25,10 @@
 
 #include "hegjoin_b200.h"
 
+namespace hj {
+void result_set_stream(hj_result* r, cudaStream_t s);   // hj_join.cu
+}
+
 namespace {
 
 double now_s() {
@@ -123,6 +127,9 @@ void worker_main(hj_server* S) {
         if (s != HJ_OK && !r->err[0]) snprintf(r->err, sizeof(r->err), "%s", hj_last_error());
         if (ix) hj_index_destroy(ix);
         cudaStreamSynchronize(st);
+        // the worker's stream dies with the server; the finished result's later
+        // frees go to the legacy default stream (all its work is complete)
+        if (r->result) hj::result_set_stream(r->result, nullptr);
         {
             std::lock_guard<std::mutex> lk(S->mu);
             r->status = s;

@@ -166,7 +166,8 @@ hj_status hj_workload_export(const hj_index* ix, hj_scheduling_cell* d_sched,
 void hj_join_opts_default(hj_join_opts* o);
 /* Runs estimator, batches, refine and result grouping.  The result keeps, per
  * batch, the neighbour ids grouped by query (device memory) plus a device
- * neighbour table of n entries.  Synchronises `stream`. */
+ * neighbour table of n entries.  Synchronises `stream`.  The result's memory is
+ * released in the order of `stream`, which must outlive the result. */
 hj_status hj_join(hj_index* ix, const hj_join_opts* opts, void* stream, hj_result** out,
                   hj_join_stats* stats);
 hj_status hj_result_destroy(hj_result* r);
@@ -225,7 +226,8 @@ hj_status hj_server_submit(hj_server* s, const void* h_db, uint32_t n, uint32_t 
                            double eps, uint64_t* ticket);
 /* Blocks until the request is done (or timeout_s passes: HJ_ERR_TIMEOUT).
  * The result (device memory) passes to the caller when `result` is non-NULL,
- * else it is released. */
+ * else it is released; it is tied to the legacy default stream, so it may
+ * outlive the server. */
 hj_status hj_server_wait(hj_server* s, uint64_t ticket, double timeout_s, hj_result** result,
                          hj_serve_info* info);
 hj_status hj_server_destroy(hj_server* s);
