@@ -132,6 +132,21 @@ hj_status hj_grid_geometry(const void* d_db, uint32_t n, uint32_t d, uint32_t k,
                            double eps, double* h_min_arr, double* h_max_arr,
                            uint32_t* h_n_cells, uint64_t* h_total_cells, void* stream);
 
+/* The same geometry without any device allocation; it has no counterpart in
+ * the reference.  For callers that cannot allocate device memory where they
+ * need the geometry: a process that reserves all of its device memory up
+ * front and must not fail on an allocation later, or code running while a
+ * stream is being captured (cudaMalloc is not allowed then).  Its scratch is a
+ * file-scope device array of 151,808 bytes (k <= 16 indexed dimensions, any
+ * n) that every GPU loading the library keeps until exit; larger k is rejected
+ * with HJ_ERR_INVALID.  All calls on a device share that array, so calls that
+ * overlap on the GPU race: serialise them.  The first call on a device looks
+ * up the array's address; make it before any stream capture.  Synchronises
+ * `stream`. */
+hj_status hj_grid_geometry_noalloc(const void* d_db, uint32_t n, uint32_t d, uint32_t k, int dtype,
+                                   double eps, double* h_min_arr, double* h_max_arr,
+                                   uint32_t* h_n_cells, uint64_t* h_total_cells, void* stream);
+
 /* ---- index build: replaces gridIndexingGPU (GPU.cu:74-398, GPU.h:9-27) ----- */
 /* d_db: n x d row-major dataset on the device (float or double per dtype).
  * h_min_arr / h_n_cells: the grid geometry (k entries); NULL = compute it with
