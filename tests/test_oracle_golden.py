@@ -1,7 +1,8 @@
 """Pins the CPU oracle to the reference itself.
 
 tests/golden/*.npz were produced by running the reference's own GPU-only join
-(compiled unmodified from its sources, oracle/ref/) on seeded datasets; see
+(compiled from its sources by oracle/ref/, with its cell-lookup comparator made
+callable on the device) on seeded datasets; see
 tests/golden/make_ref_fixtures.py.  Every integer output of the oracle must
 match what the reference computed, bit for bit.
 """
