@@ -6,7 +6,7 @@
 // is a GEMM on the 5th-generation tensor cores:
 //
 //   A (M = 128 candidates, streamed by TMA) = [-2 c~, 1, 1, |c~|^2_hi, |c~|^2_lo, 0...]
-//   B (N = 4 x 128 queries, resident)       = [  q~, |q~|^2_hi, |q~|^2_lo, 1, 1, 0...]
+//   B (N = 2 x 256 queries, resident)       = [  q~, |q~|^2_hi, |q~|^2_lo, 1, 1, 0...]
 //   D = A B^T = |q~|^2 + |c~|^2 - 2 q~.c~ = |q~ - c~|^2        (FP32 accumulate in TMEM)
 //
 // where x~ is the FP16 (or BF16) rounding of x - origin.  The norms ride in the
@@ -20,14 +20,18 @@
 // accumulation error and the reference's own FP32 rounding; derivation in
 // tc_delta_row below).  The result set is therefore identical to the exact path.
 //
-// Kernel shape (one CTA per SM, persistent, 192 threads):
-//   warp 0      TMA producer: query tiles once per work item, candidate tiles
-//               through a ring of shared-memory stages;
-//   warp 1      MMA issuer: per candidate tile, 4 MMAs (one per query tile) into
-//               4 TMEM accumulators of 128 columns (all 512 TMEM columns);
-//   warps 2..5  epilogue: tcgen05.ld 32 columns at a time, min-reduce, compare,
-//               warp-aggregated emission; releases an accumulator as soon as it
-//               has been read, so MMA and epilogue overlap across accumulators.
+// Kernel shape (one CTA per SM, persistent, 64 + 128 * EPI threads):
+//   warp 0      TMA producer: the query block once per work item, candidate
+//               tiles through a ring of shared-memory stages;
+//   warp 1      MMA issuer: per candidate tile, M = 128 x N = 256 MMAs into 2
+//               TMEM accumulators of 256 columns (all 512 TMEM columns), one per
+//               half of the query block.  N = 256 matters: a microbenchmark of
+//               this pattern issued 128 x 128 x 16 MMAs at 42% of the tensor
+//               pipe's rate and 128 x 256 x 16 ones at 98%;
+//   warps 2..   epilogue, EPI groups of 4 warps (one per TMEM lane quarter):
+//               tcgen05.ld, min-reduce, compare, warp-aggregated emission; an
+//               accumulator is released as soon as it has been read, so MMA
+//               and epilogue overlap.
 // Every wait is bounded; a timeout raises an error flag, drains and returns.
 
 #include <cudaTypedefs.h>
@@ -43,12 +47,15 @@
 namespace hj {
 namespace {
 
-constexpr int kQT = 4;                       // query tiles per work item
-constexpr int kTileRows = 128;               // rows per tile (M for A, N for B)
+constexpr int kQT = 4;                       // 128-row query loads per work item
+constexpr int kTileRows = 128;               // rows per tile (M for A) and per query load
 constexpr int kQB = kQT * kTileRows;         // queries per work item
+constexpr int kAcc = 2;                      // TMEM accumulators (query halves) per work item
+constexpr int kAccCols = 256;                // N of one MMA: queries per accumulator
 constexpr int kProbeThreads = 192;   // tile probe: TMA warp, MMA warp, 4 epilogue warps
 constexpr int kMaxStages = 8;
-constexpr uint32_t kKBlockBytes = kTileRows * 64;   // one 32-element K block of a tile
+constexpr uint32_t kKBlockBytes = kTileRows * 64;   // one 32-element K block of a 128-row tile
+constexpr uint32_t kBKBlockBytes = kQB * 64;        // one 32-element K block of the whole query block
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMaxRanges = 256;
 constexpr long long kWaitCycles = 4000000000ll;     // ~2 s at 1.9 GHz
@@ -82,8 +89,8 @@ struct TcArgs {
 struct TcShared {
     uint64_t full_a[kMaxStages];
     uint64_t empty_a[kMaxStages];
-    uint64_t full_acc[kQT];
-    uint64_t empty_acc[kQT];
+    uint64_t full_acc[kAcc];
+    uint64_t empty_acc[kAcc];
     uint64_t bfull;
     uint32_t tmem_base;
     uint32_t item;
@@ -105,14 +112,18 @@ __device__ __forceinline__ uint32_t lower_bound_lid(const unsigned long long* a,
     return lo;
 }
 
-__device__ __forceinline__ uint32_t tile_range(const TcShared& S, uint32_t t) {
-    uint32_t lo = 0, hi = S.nr;   // last r with tp[r] <= t
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (S.tp[mid] <= t) lo = mid; else hi = mid;
+// Tiles are visited in order, so the range of tile t is found by walking r
+// forward from the previous tile's range (the last r with tp[r] <= t; ranges
+// without tiles are stepped over) instead of a binary search per tile.
+struct TileWalk {
+    uint32_t r = 0, start = 0, valid = 0;
+    __device__ __forceinline__ void locate(const TcShared& S, uint32_t t) {
+        while (r + 1 < S.nr && S.tp[r + 1] <= t) ++r;
+        const uint32_t off = (t - S.tp[r]) * kTileRows;
+        start = S.rs[r] + off;
+        valid = min((uint32_t)kTileRows, S.rl[r] - off);
     }
-    return lo;
-}
+};
 
 // delta for one candidate row against the whole query block (all bounds rounded up):
 //   |D - d2_ref| <= acc + res + e (2 sT + 3 e) + ref_rel (sT + e)^2
@@ -151,8 +162,8 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
     uint32_t base = tc::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (base & 1023u)) & 1023u);
     const uint32_t tile_bytes = a.nkb * kKBlockBytes;
-    uint8_t* b_tiles = smem;                                   // kQT tiles
-    uint8_t* a_tiles = smem + kQT * tile_bytes;                // a.stages tiles
+    uint8_t* b_tiles = smem;                                   // query block: [K block][512 rows]
+    uint8_t* a_tiles = smem + kQT * tile_bytes;                // a.stages tiles: [K block][128 rows]
     TcShared& S = *reinterpret_cast<TcShared*>(a_tiles + a.stages * tile_bytes);
 
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
@@ -161,7 +172,7 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
             tc::mbar_init(&S.full_a[s], 1);
             tc::mbar_init(&S.empty_a[s], 1);
         }
-        for (int j = 0; j < kQT; ++j) {
+        for (int j = 0; j < kAcc; ++j) {
             tc::mbar_init(&S.full_acc[j], 1);
             tc::mbar_init(&S.empty_acc[j], 4 * EPI);
         }
@@ -183,7 +194,7 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
 
     // role state carried across work items (barrier phases)
     uint32_t it = 0;            // candidate tiles issued / consumed
-    uint32_t acc_use[kQT] = {0, 0, 0, 0};
+    uint32_t acc_use[kAcc] = {0, 0};
     uint32_t items_loaded = 0;
     WarpChunk wc_acc, wc_band;
     warp_chunk_init(wc_acc);
@@ -282,7 +293,7 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
                 S.ntiles = incl;
                 S.nr = nr;
                 S.nq = nq;
-                S.nqt = (nq + kTileRows - 1) / kTileRows;
+                S.nqt = (nq + kAccCols - 1) / kAccCols;   // accumulators in use
                 S.q0 = blk.q0;
             }
         }
@@ -293,20 +304,23 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
         if (warp == 0) {
             if (lane == 0) {
                 // ---------------- TMA producer
-                tc::mbar_arrive_expect_tx(&S.bfull, nqt * tile_bytes);
-                for (uint32_t j = 0; j < nqt; ++j)
+                // every row an accumulator's MMA reads is loaded (rows past n are zero-filled)
+                const uint32_t nloads = nqt * (kAccCols / kTileRows);
+                tc::mbar_arrive_expect_tx(&S.bfull, nloads * tile_bytes);
+                for (uint32_t j = 0; j < nloads; ++j)
                     for (uint32_t kb = 0; kb < a.nkb; ++kb)
-                        tc::tma_load_2d(b_tiles + j * tile_bytes + kb * kKBlockBytes, &tm_query, &S.bfull,
+                        tc::tma_load_2d(b_tiles + kb * kBKBlockBytes + j * kKBlockBytes, &tm_query, &S.bfull,
                                         (int)(kb * 32), (int)(blk.q0 + j * kTileRows));
-                for (uint32_t t = 0; t < ntiles; ++t, ++it) {
+                TileWalk tw;
+                for (uint32_t t = 0; t < ntiles; ++t) {
                     const uint32_t s = it % a.stages, use = it / a.stages;
                     if (use > 0 && !tc::mbar_wait(&S.empty_a[s], (use - 1) & 1u, abort, a.err, kWaitCycles)) break;
-                    const uint32_t r = tile_range(S, t);
-                    const uint32_t start = S.rs[r] + (t - S.tp[r]) * kTileRows;
+                    tw.locate(S, t);
                     tc::mbar_arrive_expect_tx(&S.full_a[s], tile_bytes);
                     for (uint32_t kb = 0; kb < a.nkb; ++kb)
                         tc::tma_load_2d(a_tiles + s * tile_bytes + kb * kKBlockBytes, &tm_cand, &S.full_a[s],
-                                        (int)(kb * 32), (int)start);
+                                        (int)(kb * 32), (int)tw.start);
+                    ++it;
                 }
             }
             __syncwarp();
@@ -318,7 +332,7 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
                 tc::fence_after();
                 const uint32_t ksteps = a.nkb * 2;
                 const uint32_t a_base = tc::smem_u32(a_tiles), b_base = tc::smem_u32(b_tiles);
-                for (uint32_t t = 0; ok && t < ntiles; ++t, ++it) {
+                for (uint32_t t = 0; ok && t < ntiles; ++t) {
                     const uint32_t s = it % a.stages, use = it / a.stages;
                     if (!tc::mbar_wait(&S.full_a[s], use & 1u, abort, a.err, kWaitCycles)) break;
                     tc::fence_after();
@@ -329,45 +343,62 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
                             break;
                         }
                         tc::fence_after();
+                        // M = 128 candidates x N = 256 queries per MMA: the shape that keeps the
+                        // tensor pipe busy (N = 128 MMAs issue at well under half its rate)
                         for (uint32_t ks = 0; ks < ksteps; ++ks) {
-                            const uint32_t koff = (ks >> 1) * kKBlockBytes + (ks & 1u) * 32u;
-                            uint64_t ad = tc::desc_kmajor_sw64(a_base + s * tile_bytes + koff);
-                            uint64_t bd = tc::desc_kmajor_sw64(b_base + j * tile_bytes + koff);
-                            tc::mma_f16(tmem + j * kTileRows, ad, bd, a.idesc, ks > 0 ? 1u : 0u);
+                            const uint32_t kin = (ks & 1u) * 32u;
+                            uint64_t ad = tc::desc_kmajor_sw64(a_base + s * tile_bytes + (ks >> 1) * kKBlockBytes + kin);
+                            uint64_t bd = tc::desc_kmajor_sw64(b_base + (ks >> 1) * kBKBlockBytes +
+                                                               j * (kAccCols * 64u) + kin);
+                            tc::mma_f16(tmem + j * kAccCols, ad, bd, a.idesc, ks > 0 ? 1u : 0u);
                         }
                         tc::mma_commit(&S.full_acc[j]);
                         ++acc_use[j];
                     }
                     tc::mma_commit(&S.empty_a[s]);
+                    ++it;
                 }
             }
             __syncwarp();
             it = __shfl_sync(0xffffffffu, it, 0);
 #pragma unroll
-            for (int j = 0; j < kQT; ++j) acc_use[j] = __shfl_sync(0xffffffffu, acc_use[j], 0);
+            for (int j = 0; j < kAcc; ++j) acc_use[j] = __shfl_sync(0xffffffffu, acc_use[j], 0);
             ++items_loaded;
         } else {
             // ---------------- epilogue: warps 2 .. 2 + 4*EPI; TMEM lane quarter = warp % 4,
-            // column group = (warp - 2) / 4 (128 / EPI columns of each accumulator)
+            // column group = (warp - 2) / 4 (256 / EPI columns of each accumulator)
             const uint32_t quarter = warp & 3u;
             const uint32_t grp = (warp - 2) >> 2;
             const uint32_t row = quarter * 32u + lane;
             const uint32_t lane_base = (quarter * 32u) << 16;
-            const float me = __uint_as_float(S.max_e), mn = __uint_as_float(S.max_n), mr = __uint_as_float(S.max_r);
-            unsigned long long n_acc = 0, n_band = 0;
+            // per-thread pair counts of one launch stay far below 2^32 (bounded by the sink)
+            uint32_t n_acc = 0, n_band = 0;
             bool ok = true;
+            // this warp's columns of an accumulator: COLS = 256 / EPI, read in chunks of
+            // LDW by tcgen05.ld, W chunks per wait ("wave"); the accumulator is handed
+            // back once the last wave is in registers.  EPI 4 (96 registers a thread)
+            // reads both of its 32-column chunks in one wave.
+            constexpr uint32_t COLS = kAccCols / EPI;
+            constexpr uint32_t LDW = EPI == 4 ? 32u : 64u;
+            constexpr uint32_t NCH = COLS / LDW;
+            constexpr uint32_t W = EPI == 4 ? 2u : 1u;
+            TileWalk tw;
+            tw.locate(S, 0);
+            float4 pc = row < tw.valid ? a.pinfo[tw.start + row] : make_float4(0.f, 0.f, 0.f, 0.f);
             for (uint32_t t = 0; ok && t < ntiles; ++t) {
-                const uint32_t r = tile_range(S, t);
-                const uint32_t off = (t - S.tp[r]) * kTileRows;
-                const uint32_t start = S.rs[r] + off;
-                const uint32_t valid = min((uint32_t)kTileRows, S.rl[r] - off);
-                const bool vrow = row < valid;
-                const uint32_t cpos = start + row;
+                const uint32_t cpos = tw.start + row;
+                const bool vrow = row < tw.valid;
                 float hi = -INFINITY, lo = -INFINITY;
                 if (vrow) {
-                    float d = tc_delta_row(a, a.pinfo[cpos], me, mn, mr);
+                    float d = tc_delta_row(a, pc, __uint_as_float(S.max_e), __uint_as_float(S.max_n),
+                                           __uint_as_float(S.max_r));
                     hi = __fadd_ru(a.thr, d);
                     lo = __fsub_rd(a.thr, d);
+                }
+                if (t + 1 < ntiles) {
+                    // the next tile's row bounds, loaded while this tile is processed
+                    tw.locate(S, t + 1);
+                    if (row < tw.valid) pc = a.pinfo[tw.start + row];
                 }
                 uint32_t cid = 0xFFFFFFFFu;
                 for (uint32_t j = 0; j < nqt; ++j) {
@@ -376,74 +407,79 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
                         break;
                     }
                     tc::fence_after();
-                    const uint32_t ncols = min((uint32_t)kTileRows, nq - j * kTileRows);
-                    // this warp's columns of accumulator j: COLS = 128 / EPI, loaded LDW at a time
-                    constexpr uint32_t COLS = 128 / EPI;
-                    constexpr uint32_t LDW = COLS >= 64 ? 64u : 32u;
+                    const uint32_t ncols = min((uint32_t)kAccCols, nq - j * kAccCols);
 #pragma unroll
-                    for (uint32_t c0 = 0; c0 < COLS; c0 += LDW) {
-                        float v[LDW];
-                        const uint32_t col0 = grp * COLS + c0;
-                        if constexpr (LDW == 64) {
-                            tc::tmem_ld_32x64(tmem + lane_base + j * kTileRows + col0, v);
-                        } else {
-                            tc::tmem_ld_32x32(tmem + lane_base + j * kTileRows + col0, v);
+                    for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
+                        float v[W][LDW];
+#pragma unroll
+                        for (uint32_t w = 0; w < W; ++w) {
+                            const uint32_t col = grp * COLS + (c0 + w) * LDW;
+                            if constexpr (LDW == 64) {
+                                tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v[w]);
+                            } else {
+                                tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v[w]);
+                            }
                         }
                         tc::tmem_ld_wait();
-                        if (c0 + LDW >= COLS) {
+                        if (c0 + W >= NCH) {
                             // all of this warp's columns are in registers: release the accumulator
                             tc::fence_before();
                             __syncwarp();
                             if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
                         }
-                        const bool any_hit = minN<LDW>(v) <= hi;
-                        if (!__any_sync(0xffffffffu, any_hit)) continue;
 #pragma unroll
-                        for (uint32_t h = 0; h < LDW / 32; ++h) {
-                            const uint32_t cbase = col0 + h * 32u;
-                            uint32_t hmask = 0, amask = 0;
-                            if (any_hit) {
+                        for (uint32_t w = 0; w < W; ++w) {
+                            const uint32_t col0 = grp * COLS + (c0 + w) * LDW;
+                            const bool any_hit = minN<LDW>(v[w]) <= hi;
+                            if (!__any_sync(0xffffffffu, any_hit)) continue;
 #pragma unroll
-                                for (int i = 0; i < 32; ++i) {
-                                    bool inq = cbase + i < ncols;
-                                    hmask |= (uint32_t)(inq && v[h * 32 + i] <= hi) << i;
-                                    amask |= (uint32_t)(inq && v[h * 32 + i] <= lo) << i;
+                            for (uint32_t h = 0; h < LDW / 32; ++h) {
+                                const uint32_t cbase = col0 + h * 32u;
+                                uint32_t hmask = 0, amask = 0;
+                                if (any_hit) {
+#pragma unroll
+                                    for (int i = 0; i < 32; ++i) {
+                                        bool inq = cbase + i < ncols;
+                                        hmask |= (uint32_t)(inq && v[w][h * 32 + i] <= hi) << i;
+                                        amask |= (uint32_t)(inq && v[w][h * 32 + i] <= lo) << i;
+                                    }
                                 }
+                                const uint32_t bmask = hmask & ~amask;
+                                n_acc += __popc(amask);
+                                n_band += __popc(bmask);
+                                if (a.count_only) continue;
+                                if (amask && cid == 0xFFFFFFFFu) cid = a.perm[cpos];
+                                const uint32_t qcol = j * kAccCols + cbase;
+                                uint32_t m1 = amask;
+                                warp_emit(a.sink, wc_acc, __popc(amask), [&](uint32_t) {
+                                    uint32_t b = __ffs(m1) - 1;
+                                    m1 &= m1 - 1;
+                                    return make_uint2(S.qid[qcol + b], cid);
+                                });
+                                uint32_t m2 = bmask;
+                                const uint32_t q0 = S.q0;
+                                warp_emit(a.band, wc_band, __popc(bmask), [&](uint32_t) {
+                                    uint32_t b = __ffs(m2) - 1;
+                                    m2 &= m2 - 1;
+                                    return make_uint2(q0 + qcol + b, cpos);
+                                });
                             }
-                            const uint32_t bmask = hmask & ~amask;
-                            n_acc += __popc(amask);
-                            n_band += __popc(bmask);
-                            if (a.count_only) continue;
-                            if (amask && cid == 0xFFFFFFFFu) cid = a.perm[cpos];
-                            const uint32_t qcol = j * kTileRows + cbase;
-                            uint32_t m1 = amask;
-                            warp_emit(a.sink, wc_acc, __popc(amask), [&](uint32_t) {
-                                uint32_t b = __ffs(m1) - 1;
-                                m1 &= m1 - 1;
-                                return make_uint2(S.qid[qcol + b], cid);
-                            });
-                            uint32_t m2 = bmask;
-                            const uint32_t q0 = S.q0;
-                            warp_emit(a.band, wc_band, __popc(bmask), [&](uint32_t) {
-                                uint32_t b = __ffs(m2) - 1;
-                                m2 &= m2 - 1;
-                                return make_uint2(q0 + qcol + b, cpos);
-                            });
                         }
                     }
                     ++acc_use[j];
                 }
             }
+            unsigned long long w_acc = n_acc, w_band = n_band;
             for (int o = 16; o > 0; o >>= 1) {
-                n_acc += __shfl_down_sync(0xffffffffu, n_acc, o);
-                n_band += __shfl_down_sync(0xffffffffu, n_band, o);
+                w_acc += __shfl_down_sync(0xffffffffu, w_acc, o);
+                w_band += __shfl_down_sync(0xffffffffu, w_band, o);
             }
             if (lane == 0) {
                 if (a.count_only) {
-                    if (n_acc + n_band) atomicAdd(&a.block_counts[item], n_acc + n_band);
+                    if (w_acc + w_band) atomicAdd(&a.block_counts[item], w_acc + w_band);
                 } else if (a.stats) {
-                    if (n_acc) atomicAdd(&a.stats[0], n_acc);
-                    if (n_band) atomicAdd(&a.stats[1], n_band);
+                    if (w_acc) atomicAdd(&a.stats[0], w_acc);
+                    if (w_band) atomicAdd(&a.stats[1], w_band);
                 }
             }
             it += ntiles;
@@ -592,7 +628,7 @@ __global__ void __launch_bounds__(kProbeThreads, 1)
         for (uint32_t kb = 0; kb < nkb; ++kb) {
             tc::tma_load_2d(a_tile + kb * kKBlockBytes, &tm_cand, &bars[0], (int)(kb * 32), (int)a0);
             for (uint32_t j = 0; j < kQT; ++j)
-                tc::tma_load_2d(b_tiles + j * tile_bytes + kb * kKBlockBytes, &tm_query, &bars[0], (int)(kb * 32),
+                tc::tma_load_2d(b_tiles + kb * kBKBlockBytes + j * kKBlockBytes, &tm_query, &bars[0], (int)(kb * 32),
                                 (int)(b0 + j * kTileRows));
         }
     }
@@ -600,12 +636,14 @@ __global__ void __launch_bounds__(kProbeThreads, 1)
         bool ok = tc::mbar_wait(&bars[0], 0, abortp, err, kWaitCycles);
         tc::fence_after();
         if (ok) {
-            for (uint32_t j = 0; j < kQT; ++j)
+            for (uint32_t j = 0; j < kAcc; ++j)
                 for (uint32_t ks = 0; ks < nkb * 2; ++ks) {
-                    const uint32_t koff = (ks >> 1) * kKBlockBytes + (ks & 1u) * 32u;
-                    tc::mma_f16(tmem + j * kTileRows, tc::desc_kmajor_sw64(tc::smem_u32(a_tile) + koff),
-                                tc::desc_kmajor_sw64(tc::smem_u32(b_tiles) + j * tile_bytes + koff), idesc,
-                                ks > 0 ? 1u : 0u);
+                    const uint32_t kin = (ks & 1u) * 32u;
+                    tc::mma_f16(tmem + j * kAccCols,
+                                tc::desc_kmajor_sw64(tc::smem_u32(a_tile) + (ks >> 1) * kKBlockBytes + kin),
+                                tc::desc_kmajor_sw64(tc::smem_u32(b_tiles) + (ks >> 1) * kBKBlockBytes +
+                                                     j * (kAccCols * 64u) + kin),
+                                idesc, ks > 0 ? 1u : 0u);
                 }
         }
         tc::mma_commit(&bars[1]);
@@ -805,7 +843,7 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     a.ref_rel = (float)((ix->d + 2) * std::ldexp(1.0, -24) * 1.01);
     a.sink = sink; a.band = band;
     a.count_only = count_only; a.block_counts = block_counts; a.stats = stats; a.err = err;
-    a.idesc = tc::idesc_f16(ix->tc_kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kTileRows);
+    a.idesc = tc::idesc_f16(ix->tc_kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kAccCols);
     unsigned grid = (unsigned)std::min<uint32_t>((uint32_t)num_sms(), nblocks);
     kern<<<grid, 64 + 128 * epi, smem, st>>>(s->maps.cand, s->maps.query, a);
     HJ_LAUNCHED();
@@ -839,7 +877,7 @@ extern "C" hj_status hj_probe_tc_tile(hj_index* ix, int kind, uint32_t a0, uint3
     HJ_TRY(dalloc(&err, 1, st));
     HJ_CUDA(cudaMemsetAsync(err, 0, 4, st));
     k_tc_tile_probe<<<1, kProbeThreads, smem, st>>>(s->maps.cand, s->maps.query, nkb,
-                                               tc::idesc_f16(kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kTileRows),
+                                               tc::idesc_f16(kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kAccCols),
                                                a0, b0, d_out, err);
     HJ_LAUNCHED();
     uint32_t herr = 0;

@@ -32,29 +32,45 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// try_wait with a suspend-time hint: a waiting thread sleeps (up to the hint)
-// until the phase completes instead of spinning on the barrier.
+// try_wait, optionally with a suspend-time hint (a waiting thread sleeps, up to
+// the hint, until the phase completes).  Measured on B200: alone, a hinted
+// try_wait on an already completed phase delays the MMAs issued after it by
+// ~160 cycles; but in the full kernel, unhinted spinning by the TMA and MMA
+// threads took issue slots from the epilogue warps and was slower overall, so
+// every role sleeps.
+template <bool kSleep>
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
-        : "memory");
+    if constexpr (kSleep) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+    }
     return ok != 0;
 }
 
 // Bounded wait: gives up after ~`limit_cycles` SM cycles or when *abort is
 // raised by another role, records the timeout in *err and returns false.
+template <bool kSleep = true>
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile uint32_t* abort,
                                           uint32_t* err, long long limit_cycles) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait<kSleep>(bar, parity)) return true;
     long long t0 = clock64();
     uint32_t spins = 0;
     while (true) {
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait<kSleep>(bar, parity)) return true;
         if ((++spins & 255u) == 0) {
             if (*abort) return false;
             if (clock64() - t0 > limit_cycles) {
