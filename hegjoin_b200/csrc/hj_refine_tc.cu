@@ -20,15 +20,16 @@
 // accumulation error and the reference's own FP32 rounding; derivation in
 // tc_delta_row below).  The result set is therefore identical to the exact path.
 //
-// Kernel shape (one CTA per SM, persistent, 64 + 128 * EPI threads):
+// Kernel shape (one CTA per SM, persistent, 96 + 128 * EPI threads):
 //   warp 0      TMA producer: the query block once per work item, candidate
 //               tiles through a ring of shared-memory stages;
-//   warp 1      MMA issuer: per candidate tile, M = 128 x N = 256 MMAs into 2
-//               TMEM accumulators of 256 columns (all 512 TMEM columns), one per
-//               half of the query block.  N = 256 matters: a microbenchmark of
-//               this pattern issued 128 x 128 x 16 MMAs at 42% of the tensor
-//               pipe's rate and 128 x 256 x 16 ones at 98%;
-//   warps 2..   epilogue, EPI groups of 4 warps (one per TMEM lane quarter):
+//   warps 1, 2  MMA issuers, one per TMEM accumulator: per candidate tile,
+//               M = 128 x N = 256 MMAs into 2 accumulators of 256 columns (all
+//               512 TMEM columns), one per half of the query block.  N = 256
+//               matters: a microbenchmark of this pattern issued 128 x 128 x 16
+//               MMAs at 42% of the tensor pipe's rate and 128 x 256 x 16 ones at
+//               98%;
+//   warps 3..   epilogue, EPI groups of 4 warps (one per TMEM lane quarter):
 //               tcgen05.ld, min-reduce, compare, warp-aggregated emission; an
 //               accumulator is released as soon as it has been read, so MMA
 //               and epilogue overlap.
@@ -155,7 +156,7 @@ __device__ __forceinline__ float minN(const float (&v)[N]) {
 
 // EPI = epilogue warp groups (4 warps each, one per TMEM lane quarter).
 template <int EPI>
-__global__ void __launch_bounds__(64 + 128 * EPI, 1)
+__global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     k_refine_tc(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query, TcArgs a) {
     extern __shared__ uint8_t smem_raw[];
     // operand tiles need 1024-byte alignment for the swizzle pattern
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
     if (tid == 0) {
         for (uint32_t s = 0; s < a.stages; ++s) {
             tc::mbar_init(&S.full_a[s], 1);
-            tc::mbar_init(&S.empty_a[s], 1);
+            tc::mbar_init(&S.empty_a[s], kAcc);   // one arrival per MMA issuer
         }
         for (int j = 0; j < kAcc; ++j) {
             tc::mbar_init(&S.full_acc[j], 1);
@@ -325,35 +326,43 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
             }
             __syncwarp();
             it = __shfl_sync(0xffffffffu, it, 0);
-        } else if (warp == 1) {
+        } else if (warp <= kAcc) {
             if (lane == 0) {
-                // ---------------- MMA issuer
+                // ---------------- MMA issuer of accumulator h (warp 1: h = 0, warp 2: h = 1).
+                // One issuer per accumulator: every barrier wait stalls the issuing thread's
+                // MMA stream for ~160 cycles (measured), and with two issuers the other one
+                // keeps the tensor pipe busy meanwhile.  Both wait for every candidate tile
+                // and both arrive on its stage's empty barrier (count 2), so neither can run
+                // a ring cycle ahead of the other.
+                const uint32_t h = warp - 1;
                 bool ok = tc::mbar_wait(&S.bfull, items_loaded & 1u, abort, a.err, kWaitCycles);
                 tc::fence_after();
                 const uint32_t ksteps = a.nkb * 2;
                 const uint32_t a_base = tc::smem_u32(a_tiles), b_base = tc::smem_u32(b_tiles);
+                const bool active = h < nqt;
                 for (uint32_t t = 0; ok && t < ntiles; ++t) {
                     const uint32_t s = it % a.stages, use = it / a.stages;
                     if (!tc::mbar_wait(&S.full_a[s], use & 1u, abort, a.err, kWaitCycles)) break;
                     tc::fence_after();
-                    for (uint32_t j = 0; j < nqt; ++j) {
-                        if (acc_use[j] > 0 &&
-                            !tc::mbar_wait(&S.empty_acc[j], (acc_use[j] - 1) & 1u, abort, a.err, kWaitCycles)) {
+                    if (active) {
+                        if (acc_use[h] > 0 &&
+                            !tc::mbar_wait(&S.empty_acc[h], (acc_use[h] - 1) & 1u, abort, a.err, kWaitCycles)) {
                             ok = false;
-                            break;
+                        } else {
+                            tc::fence_after();
+                            // M = 128 candidates x N = 256 queries per MMA: the shape that keeps
+                            // the tensor pipe busy (N = 128 MMAs issue at well under half its rate)
+                            for (uint32_t ks = 0; ks < ksteps; ++ks) {
+                                const uint32_t kin = (ks & 1u) * 32u;
+                                uint64_t ad = tc::desc_kmajor_sw64(a_base + s * tile_bytes +
+                                                                   (ks >> 1) * kKBlockBytes + kin);
+                                uint64_t bd = tc::desc_kmajor_sw64(b_base + (ks >> 1) * kBKBlockBytes +
+                                                                   h * (kAccCols * 64u) + kin);
+                                tc::mma_f16(tmem + h * kAccCols, ad, bd, a.idesc, ks > 0 ? 1u : 0u);
+                            }
+                            tc::mma_commit(&S.full_acc[h]);
+                            ++acc_use[h];
                         }
-                        tc::fence_after();
-                        // M = 128 candidates x N = 256 queries per MMA: the shape that keeps the
-                        // tensor pipe busy (N = 128 MMAs issue at well under half its rate)
-                        for (uint32_t ks = 0; ks < ksteps; ++ks) {
-                            const uint32_t kin = (ks & 1u) * 32u;
-                            uint64_t ad = tc::desc_kmajor_sw64(a_base + s * tile_bytes + (ks >> 1) * kKBlockBytes + kin);
-                            uint64_t bd = tc::desc_kmajor_sw64(b_base + (ks >> 1) * kBKBlockBytes +
-                                                               j * (kAccCols * 64u) + kin);
-                            tc::mma_f16(tmem + j * kAccCols, ad, bd, a.idesc, ks > 0 ? 1u : 0u);
-                        }
-                        tc::mma_commit(&S.full_acc[j]);
-                        ++acc_use[j];
                     }
                     tc::mma_commit(&S.empty_a[s]);
                     ++it;
@@ -365,10 +374,10 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
             for (int j = 0; j < kAcc; ++j) acc_use[j] = __shfl_sync(0xffffffffu, acc_use[j], 0);
             ++items_loaded;
         } else {
-            // ---------------- epilogue: warps 2 .. 2 + 4*EPI; TMEM lane quarter = warp % 4,
-            // column group = (warp - 2) / 4 (256 / EPI columns of each accumulator)
+            // ---------------- epilogue: warps 3 .. 3 + 4*EPI; TMEM lane quarter = warp % 4,
+            // column group = (warp - 3) / 4 (256 / EPI columns of each accumulator)
             const uint32_t quarter = warp & 3u;
-            const uint32_t grp = (warp - 2) >> 2;
+            const uint32_t grp = (warp - 1 - kAcc) >> 2;
             const uint32_t row = quarter * 32u + lane;
             const uint32_t lane_base = (quarter * 32u) << 16;
             // per-thread pair counts of one launch stay far below 2^32 (bounded by the sink)
@@ -384,7 +393,15 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
             constexpr uint32_t W = EPI == 4 ? 2u : 1u;
             TileWalk tw;
             tw.locate(S, 0);
-            float4 pc = row < tw.valid ? a.pinfo[tw.start + row] : make_float4(0.f, 0.f, 0.f, 0.f);
+            // the row's bounds and original id, loaded one tile ahead: a global load on the
+            // hit path stalls the warp, and a stalled warp holds back the release of the
+            // next accumulator
+            float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+            uint32_t cid_next = 0u;
+            if (row < tw.valid) {
+                pc = a.pinfo[tw.start + row];
+                if (!a.count_only) cid_next = a.perm[tw.start + row];
+            }
             for (uint32_t t = 0; ok && t < ntiles; ++t) {
                 const uint32_t cpos = tw.start + row;
                 const bool vrow = row < tw.valid;
@@ -398,9 +415,12 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
                 if (t + 1 < ntiles) {
                     // the next tile's row bounds, loaded while this tile is processed
                     tw.locate(S, t + 1);
-                    if (row < tw.valid) pc = a.pinfo[tw.start + row];
                 }
-                uint32_t cid = 0xFFFFFFFFu;
+                const uint32_t cid = cid_next;
+                if (t + 1 < ntiles && row < tw.valid) {
+                    pc = a.pinfo[tw.start + row];
+                    if (!a.count_only) cid_next = a.perm[tw.start + row];
+                }
                 for (uint32_t j = 0; j < nqt; ++j) {
                     if (!tc::mbar_wait(&S.full_acc[j], acc_use[j] & 1u, abort, a.err, kWaitCycles)) {
                         ok = false;
@@ -448,7 +468,6 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
                                 n_acc += __popc(amask);
                                 n_band += __popc(bmask);
                                 if (a.count_only) continue;
-                                if (amask && cid == 0xFFFFFFFFu) cid = a.perm[cpos];
                                 const uint32_t qcol = j * kAccCols + cbase;
                                 uint32_t m1 = amask;
                                 warp_emit(a.sink, wc_acc, __popc(amask), [&](uint32_t) {
@@ -485,7 +504,7 @@ __global__ void __launch_bounds__(64 + 128 * EPI, 1)
             it += ntiles;
         }
     }
-    if (warp >= 2 && !a.count_only) {
+    if (warp > kAcc && !a.count_only) {
         warp_chunk_close(a.sink, wc_acc);
         warp_chunk_close(a.band, wc_band);
     }
@@ -845,7 +864,7 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     a.count_only = count_only; a.block_counts = block_counts; a.stats = stats; a.err = err;
     a.idesc = tc::idesc_f16(ix->tc_kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kAccCols);
     unsigned grid = (unsigned)std::min<uint32_t>((uint32_t)num_sms(), nblocks);
-    kern<<<grid, 64 + 128 * epi, smem, st>>>(s->maps.cand, s->maps.query, a);
+    kern<<<grid, 32 * (1 + kAcc) + 128 * epi, smem, st>>>(s->maps.cand, s->maps.query, a);
     HJ_LAUNCHED();
     return HJ_OK;
 }
