@@ -383,7 +383,8 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         const std::string key = tune_key(refine, ix->d, ix->dtype);
         if (tc && !tune_lookup(key, &tuned) && tuning_enabled()) {
             // time each epilogue width on the sample; the last run's counts are the estimate
-            const int cands[3] = {1, 2, 4};
+            // epilogue shapes: warp groups | 8 * (one warp set per accumulator)
+            const int cands[4] = {2, 4, 10, 12};
             float best = 1e30f;
             int best_epi = tc_get_epi(ix);
             cudaEvent_t e0, e1;

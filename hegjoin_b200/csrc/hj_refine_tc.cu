@@ -29,10 +29,11 @@
 //               matters: a microbenchmark of this pattern issued 128 x 128 x 16
 //               MMAs at 42% of the tensor pipe's rate and 128 x 256 x 16 ones at
 //               98%;
-//   warps 3..   epilogue, EPI groups of 4 warps (one per TMEM lane quarter):
-//               tcgen05.ld, min-reduce, compare, warp-aggregated emission; an
-//               accumulator is released as soon as it has been read, so MMA
-//               and epilogue overlap.
+//   warps 3..   epilogue, EPI groups of 4 warps (one per TMEM lane quarter),
+//               either all draining both accumulators or split into one set per
+//               accumulator (autotuned): tcgen05.ld, min-reduce, compare,
+//               warp-aggregated emission; an accumulator is released as soon as
+//               its set has read it, so MMA and epilogue overlap.
 // Every wait is bounded; a timeout raises an error flag, drains and returns.
 
 #include <cudaTypedefs.h>
@@ -141,23 +142,37 @@ __device__ __forceinline__ float tc_delta_row(const TcArgs& a, float4 pc, float 
     return d * 1.01f + 1e-30f;
 }
 
-// Tree minimum of N values (depth log2 N, so the epilogue's compare is not a dependent chain).
+// Tree minimum of N values with three-input minima.
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
 template <uint32_t N>
 __device__ __forceinline__ float minN(const float (&v)[N]) {
-    float m[N / 2];
+    if constexpr (N == 1) {
+        return v[0];
+    } else if constexpr (N == 2) {
+        return fminf(v[0], v[1]);
+    } else {
+        constexpr uint32_t M = (N + 2) / 3;
+        float m[M];
 #pragma unroll
-    for (uint32_t i = 0; i < N / 2; ++i) m[i] = fminf(v[2 * i], v[2 * i + 1]);
-#pragma unroll
-    for (uint32_t w = N / 4; w >= 1; w >>= 1)
-#pragma unroll
-        for (uint32_t i = 0; i < w; ++i) m[i] = fminf(m[2 * i], m[2 * i + 1]);
-    return m[0];
+        for (uint32_t i = 0; i < N / 3; ++i) m[i] = fmin3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        if constexpr (N % 3 == 1) m[M - 1] = v[N - 1];
+        if constexpr (N % 3 == 2) m[M - 1] = fminf(v[N - 2], v[N - 1]);
+        return minN<M>(m);
+    }
 }
 
-// EPI = epilogue warp groups (4 warps each, one per TMEM lane quarter).
-template <int EPI>
+// EPI = epilogue warp groups (4 warps each, one per TMEM lane quarter).  SPLIT:
+// the epilogue warps form one set per accumulator (a warp drains half as many
+// accumulators, each over a whole tile's MMA time) instead of every warp draining
+// both.  Which is faster depends on d: the autotuner times all four shapes.
+template <int EPI, bool SPLIT>
 __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     k_refine_tc(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query, TcArgs a) {
+    static_assert(EPI == 2 || EPI == 4, "an epilogue set needs whole groups of 4 warps");
     extern __shared__ uint8_t smem_raw[];
     // operand tiles need 1024-byte alignment for the swizzle pattern
     uint32_t base = tc::smem_u32(smem_raw);
@@ -175,7 +190,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
         }
         for (int j = 0; j < kAcc; ++j) {
             tc::mbar_init(&S.full_acc[j], 1);
-            tc::mbar_init(&S.empty_acc[j], 4 * EPI);
+            tc::mbar_init(&S.empty_acc[j], SPLIT ? 2 * EPI : 4 * EPI);   // the warps draining it
         }
         tc::mbar_init(&S.bfull, 1);
         S.abort = 0;
@@ -195,7 +210,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
 
     // role state carried across work items (barrier phases)
     uint32_t it = 0;            // candidate tiles issued / consumed
-    uint32_t acc_use[kAcc] = {0, 0};
+    uint32_t acc_use[kAcc] = {0, 0};   // uses of each accumulator seen by this thread
     uint32_t items_loaded = 0;
     WarpChunk wc_acc, wc_band;
     warp_chunk_init(wc_acc);
@@ -374,23 +389,29 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
             for (int j = 0; j < kAcc; ++j) acc_use[j] = __shfl_sync(0xffffffffu, acc_use[j], 0);
             ++items_loaded;
         } else {
-            // ---------------- epilogue: warps 3 .. 3 + 4*EPI; TMEM lane quarter = warp % 4,
-            // column group = (warp - 3) / 4 (256 / EPI columns of each accumulator)
+            // ---------------- epilogue: warps 3 .. 3 + 4*EPI.  SPLIT: two sets of 2*EPI warps,
+            // one per accumulator, so a warp has a whole tile's MMA time to drain its share
+            // of one accumulator and a slow warp holds back only its own accumulator;
+            // otherwise one set of 4*EPI warps drains both.  TMEM lane quarter = warp % 4;
+            // column group within the set = (index in set) / 4.
+            constexpr uint32_t SETW = SPLIT ? 2 * EPI : 4 * EPI;
+            const uint32_t ew = warp - 1 - kAcc;
+            const uint32_t hset = ew / SETW;   // SPLIT: the accumulator this warp drains
             const uint32_t quarter = warp & 3u;
-            const uint32_t grp = (warp - 1 - kAcc) >> 2;
+            const uint32_t grp = (ew % SETW) >> 2;
             const uint32_t row = quarter * 32u + lane;
             const uint32_t lane_base = (quarter * 32u) << 16;
             // per-thread pair counts of one launch stay far below 2^32 (bounded by the sink)
             uint32_t n_acc = 0, n_band = 0;
             bool ok = true;
-            // this warp's columns of an accumulator: COLS = 256 / EPI, read in chunks of
-            // LDW by tcgen05.ld, W chunks per wait ("wave"); the accumulator is handed
-            // back once the last wave is in registers.  EPI 4 (96 registers a thread)
-            // reads both of its 32-column chunks in one wave.
-            constexpr uint32_t COLS = kAccCols / EPI;
+            // this warp's columns of an accumulator: COLS = 256 / (SETW / 4), read in chunks
+            // of LDW by tcgen05.ld, W chunks per wait ("wave"); the accumulator is handed back
+            // once the last wave is in registers.  EPI 4 leaves 96 registers a thread: two
+            // 32-column chunks per wave when a warp has 64 columns, one when it has 128.
+            constexpr uint32_t COLS = kAccCols / (SETW / 4);
             constexpr uint32_t LDW = EPI == 4 ? 32u : 64u;
             constexpr uint32_t NCH = COLS / LDW;
-            constexpr uint32_t W = EPI == 4 ? 2u : 1u;
+            constexpr uint32_t W = (EPI == 4 && !SPLIT) ? 2u : 1u;
             TileWalk tw;
             tw.locate(S, 0);
             // the row's bounds and original id, loaded one tile ahead: a global load on the
@@ -421,14 +442,15 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                     pc = a.pinfo[tw.start + row];
                     if (!a.count_only) cid_next = a.perm[tw.start + row];
                 }
-                for (uint32_t j = 0; j < nqt; ++j) {
+                const uint32_t j_end = SPLIT ? min(hset + 1, nqt) : nqt;
+                for (uint32_t j = SPLIT ? hset : 0u; j < j_end; ++j) {
                     if (!tc::mbar_wait(&S.full_acc[j], acc_use[j] & 1u, abort, a.err, kWaitCycles)) {
                         ok = false;
                         break;
                     }
                     tc::fence_after();
                     const uint32_t ncols = min((uint32_t)kAccCols, nq - j * kAccCols);
-#pragma unroll
+#pragma unroll 1
                     for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
                         float v[W][LDW];
 #pragma unroll
@@ -740,7 +762,7 @@ struct TcMaps {
 
 struct TcState {
     TcMaps maps;
-    int epi = 2;              // epilogue warp groups (autotuned)
+    int epi = 4;              // epilogue shape code, EPI | 8 * SPLIT (autotuned: 2, 4, 10, 12)
     float gamma_acc = 0;
     float max_e = 0, max_n = 0, max_r = 0;
 };
@@ -827,7 +849,7 @@ int tc_get_epi(const hj_index* ix) {
 }
 void tc_set_epi(hj_index* ix, int epi) {
     TcState* s = tc_state(ix);
-    if (s && (epi == 1 || epi == 2 || epi == 4)) s->epi = epi;
+    if (s && (epi == 2 || epi == 4 || epi == 10 || epi == 12)) s->epi = epi;
 }
 
 void tc_release(hj_index* ix) {
@@ -846,11 +868,11 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     size_t smem = tc_smem_bytes(nkb, stages);
     // one CTA per SM: ask for more than half of the SM's shared memory
     smem = std::max<size_t>(smem, 116 * 1024);
-    const int epi = s->epi == 1 || s->epi == 4 ? s->epi : 2;
-    if (epi == 1) HJ_TRY(ensure_smem(k_refine_tc<1>, smem));
-    else if (epi == 2) HJ_TRY(ensure_smem(k_refine_tc<2>, smem));
-    else HJ_TRY(ensure_smem(k_refine_tc<4>, smem));
-    auto kern = epi == 1 ? k_refine_tc<1> : (epi == 2 ? k_refine_tc<2> : k_refine_tc<4>);
+    const int code = s->epi;
+    auto kern = code == 2 ? k_refine_tc<2, false>
+                          : code == 10 ? k_refine_tc<2, true> : code == 12 ? k_refine_tc<4, true> : k_refine_tc<4, false>;
+    const int epi = (code & 7) == 2 ? 2 : 4;
+    HJ_TRY(ensure_smem(kern, smem));
     TcArgs a{};
     a.blocks = blocks; a.nblocks = nblocks; a.head = head;
     a.perm = ix->perm; a.cell_lid = ix->cell_lid; a.cell_start = ix->cell_start; a.nC = ix->nC; a.grid = ix->grid;
