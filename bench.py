@@ -313,7 +313,10 @@ def compare_bench(args, wl):
             ix.close()
         sec = statistics.mean(times)
         out[refine] = {"pairs": int(st.total_pairs), "seconds_per_step": sec, "pairs_per_s": st.total_pairs / sec,
-                       "refine_kernel_ms": st.ms_refine_kernel, "band_pairs": int(st.band_pairs),
+                       "refine_kernel_ms": st.ms_refine_kernel,
+                       "join_ms": {"estimate": st.ms_estimate, "refine": st.ms_refine, "group": st.ms_group,
+                                   "total": st.ms_total},
+                       "batches": int(st.n_batches), "retries": int(st.n_retries), "band_pairs": int(st.band_pairs),
                        "tc_accepts": int(st.tc_accepts), "filter_delta": st.filter_delta,
                        "candidates": int(cand)}
     same = all(np.array_equal(a, b) for a, b in zip(digests["exact"], digests[args.tc_kind]))
