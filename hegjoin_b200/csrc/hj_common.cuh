@@ -217,4 +217,58 @@ __device__ __forceinline__ bool warp_emit(const PairSink& s, WarpChunk& c, uint3
     return ok;
 }
 
+// Append the pairs named by every lane's 32-bit hit mask, written out in
+// coalesced runs: output slot i of the warp's hits is produced by lane i % 32,
+// which finds the hit's owner lane (binary search over the inclusive prefix of
+// the mask counts) and its bit (n-th set bit), then calls pair_of(owner, bit).
+// Whole warp must call.  Returns false on overflow (pairs dropped; the batch
+// will be re-run).
+template <typename PairFn>
+__device__ __forceinline__ bool warp_emit_masks(const PairSink& s, WarpChunk& c, uint32_t mask, PairFn&& pair_of) {
+    if (!__any_sync(0xffffffffu, mask != 0u)) return true;
+    const uint32_t lane = lane_id();
+    const uint32_t cnt = __popc(mask);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    bool ok = true;
+    uint32_t done = 0;
+    while (done < total) {
+        uint32_t room = (c.cap != 0) ? c.cap - c.used : 0;
+        if (room == 0) {
+            if (!warp_chunk_reserve(s, c, 1)) { ok = false; break; }
+            room = c.cap - c.used;
+        }
+        const uint32_t take = min(room, total - done);
+        for (uint32_t b0 = 0; b0 < take; b0 += 32) {
+            const uint32_t r = done + b0 + lane;   // the warp-wide rank this lane writes
+            uint32_t owner = 0;                    // number of lanes whose inclusive count is <= r
+#pragma unroll
+            for (uint32_t st = 16; st > 0; st >>= 1) {
+                const uint32_t inc = __shfl_sync(0xffffffffu, incl, owner + st - 1);
+                if (inc <= r) owner += st;
+            }
+            owner = min(owner, 31u);
+            const uint32_t o_incl = __shfl_sync(0xffffffffu, incl, owner);
+            const uint32_t o_cnt = __shfl_sync(0xffffffffu, cnt, owner);
+            const uint32_t o_mask = __shfl_sync(0xffffffffu, mask, owner);
+            const uint32_t k = r - (o_incl - o_cnt);                  // the owner's k-th hit (0-based)
+            const uint32_t bit = __fns(o_mask, 0, (int)k + 1);       // 0xFFFFFFFF if there is none
+            if (b0 + lane < take && bit < 32u) {
+                const unsigned long long pos = c.base + c.used + b0 + lane;
+                const uint2 kv = pair_of(owner, bit);
+                s.keys[pos] = kv.x;
+                s.vals[pos] = kv.y;
+            }
+        }
+        c.used += take;
+        done += take;
+    }
+    return ok;
+}
+
 }  // namespace hj

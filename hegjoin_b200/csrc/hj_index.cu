@@ -217,22 +217,13 @@ __global__ void k_gather_rows(const T* __restrict__ db, const uint32_t* __restri
 }
 
 // ---- workload ------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t lower_bound_u64(const unsigned long long* a, uint32_t n, unsigned long long v) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (a[mid] < v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
 }  // namespace
 
 // Per non-empty cell: number of candidates in its stencil (kernel.cu:74-144).
 // One warp per cell; rows of the stencil (tuples over dimensions 1..k-1) are
 // split over the lanes, each row being one contiguous range of linear ids.
 __global__ void k_cell_workload(const unsigned long long* __restrict__ cell_lid, const uint32_t* __restrict__ cell_start,
-                                uint32_t nC, HjGrid grid, uint32_t* __restrict__ cell_nb,
+                                uint32_t nC, HjGrid grid, HjCellHash hash, uint32_t* __restrict__ cell_nb,
                                 unsigned long long* __restrict__ cell_work) {
     uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (warp >= nC) return;
@@ -260,11 +251,8 @@ __global__ void k_cell_workload(const unsigned long long* __restrict__ cell_lid,
                 rem /= w[j];
                 base += (unsigned long long)t * grid.mult[j];
             }
-            unsigned long long a = base + lo[0], b = a + w[0] - 1;
-            uint32_t c0 = lower_bound_u64(cell_lid, nC, a);
-            uint32_t c1 = c0;
-            while (c1 < nC && cell_lid[c1] <= b) ++c1;
-            cnt += cell_start[c1] - cell_start[c0];
+            const uint2 sp = cell_span(hash, cell_start, base + lo[0], w[0]);
+            cnt += sp.y - sp.x;
         }
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
@@ -413,8 +401,43 @@ hj_status index_create_t(const T* d_db, uint32_t n, uint32_t d, uint32_t k, T ep
     return HJ_OK;
 }
 
+__global__ void k_hash_insert(const unsigned long long* __restrict__ lid, uint32_t nC, unsigned long long* keys,
+                              uint32_t* vals, unsigned long long mask) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nC) return;
+    const unsigned long long key = lid[i];
+    unsigned long long s = mix64(key) & mask;
+    for (unsigned long long probe = 0; probe <= mask; ++probe) {   // the table is at most half full
+        const unsigned long long prev = atomicCAS(&keys[s], kEmptyLid, key);
+        if (prev == kEmptyLid || prev == key) {
+            vals[s] = i;
+            return;
+        }
+        s = (s + 1) & mask;
+    }
+}
+
+// The cell hash of an index whose cell table is built (capacity: the power of
+// two at least twice nC, at least 64).
+hj_status build_cell_hash(hj_index* ix, cudaStream_t st) {
+    unsigned long long cap = 64;
+    while (cap < 2ull * ix->nC) cap <<= 1;
+    HJ_TRY(dalloc(&ix->hash_keys, (size_t)cap, st));
+    HJ_TRY(dalloc(&ix->hash_vals, (size_t)cap, st));
+    HJ_CUDA(cudaMemsetAsync(ix->hash_keys, 0xFF, (size_t)cap * sizeof(unsigned long long), st));
+    ix->hash_mask = cap - 1;
+    if (ix->nC) {
+        k_hash_insert<<<(ix->nC + 255) / 256, 256, 0, st>>>(ix->cell_lid, ix->nC, ix->hash_keys, ix->hash_vals,
+                                                             ix->hash_mask);
+        HJ_LAUNCHED();
+    }
+    return HJ_OK;
+}
+
 void free_index(hj_index* ix, cudaStream_t st) {
     tc_release(ix);
+    dfree(ix->hash_keys, st);
+    dfree(ix->hash_vals, st);
     dfree(ix->pts, st);
     dfree(ix->perm, st);
     dfree(ix->cell_lid, st);
@@ -507,6 +530,8 @@ hj_status hj_index_create(const void* d_db, uint32_t n, uint32_t d, uint32_t k, 
     hj_status s = (dtype == HJ_F32)
                       ? index_create_t<float>((const float*)d_db, n, d, k, (float)eps, h_min_arr, h_n_cells, st, ix)
                       : index_create_t<double>((const double*)d_db, n, d, k, eps, h_min_arr, h_n_cells, st, ix);
+    // linear ids are below totalCells <= 2^64 - 1, so none equals the hash's free-slot mark
+    if (s == HJ_OK) s = build_cell_hash(ix, st);
     if (s != HJ_OK) {
         free_index(ix, st);
         cudaStreamSynchronize(st);
@@ -577,7 +602,8 @@ hj_status hj_sort_by_workload(hj_index* ix, void* stream, uint64_t* total_candid
         HJ_TRY(dalloc(&ix->cell_nb, nC, st));
         HJ_TRY(dalloc(&work, nC, st));
         unsigned g = (unsigned)(((uint64_t)nC * 32 + 255) / 256);
-        k_cell_workload<<<g, 256, 0, st>>>(ix->cell_lid, ix->cell_start, nC, ix->grid, ix->cell_nb, work);
+        k_cell_workload<<<g, 256, 0, st>>>(ix->cell_lid, ix->cell_start, nC, ix->grid, cell_hash(ix), ix->cell_nb,
+                                           work);
         HJ_LAUNCHED();
         HJ_TRY(dalloc(&dsum, 1, st));
         HJ_TRY(reduce_sum_u64(reinterpret_cast<uint64_t*>(work), nC, dsum, st));

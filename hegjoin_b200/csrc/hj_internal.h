@@ -10,6 +10,16 @@ struct HjGrid {
     unsigned long long mult[hj::kMaxK];   // mixed-radix multipliers, dimension 0 fastest
 };
 
+// Open-addressing hash of the non-empty cells, linear id -> cell index, so a
+// stencil row is found with one or two loads instead of a binary search over
+// all non-empty cells.  Capacity is a power of two at least twice nC; free
+// slots hold kEmptyLid (no cell can have that id: the index rejects it).
+struct HjCellHash {
+    const unsigned long long* keys;
+    const uint32_t* vals;
+    unsigned long long mask;   // capacity - 1
+};
+
 // Work item of the refine kernels: queries q0..q1 (sorted positions) of cell
 // `cell`, whose stencil holds `nb` candidate points.
 struct HjBlock {
@@ -37,6 +47,9 @@ struct hj_index {
     unsigned long long* cell_lid = nullptr;  // nC sorted linear ids
     uint32_t* cell_start = nullptr;  // nC + 1
     uint32_t nC = 0;
+    unsigned long long* hash_keys = nullptr;   // cell hash (HjCellHash)
+    uint32_t* hash_vals = nullptr;
+    unsigned long long hash_mask = 0;
 
     // workload (hj_sort_by_workload)
     bool have_workload = false;
@@ -68,5 +81,41 @@ void tc_release(hj_index* ix);
 // hj_index.cu
 hj_status build_blocks(const hj_index* ix, uint32_t qb, HjBlock** d_blocks, uint32_t* n_blocks,
                        cudaStream_t st);
+
+constexpr unsigned long long kEmptyLid = ~0ull;
+constexpr uint32_t kNoCell = 0xFFFFFFFFu;
+
+inline HjCellHash cell_hash(const hj_index* ix) { return HjCellHash{ix->hash_keys, ix->hash_vals, ix->hash_mask}; }
+
+// Cell index of linear id `lid`, or kNoCell.  Probes stop at a free slot; the
+// table is at most half full, so the loop ends after a few probes (and after
+// capacity probes at the very most).
+__device__ __forceinline__ uint32_t cell_find(const HjCellHash& h, unsigned long long lid) {
+    unsigned long long i = mix64(lid) & h.mask;
+    for (unsigned long long probe = 0; probe <= h.mask; ++probe) {
+        const unsigned long long key = h.keys[i];
+        if (key == lid) return h.vals[i];
+        if (key == kEmptyLid) return kNoCell;
+        i = (i + 1) & h.mask;
+    }
+    return kNoCell;
+}
+
+// Points of the existing cells with linear ids lo .. lo + w - 1 (consecutive
+// along dimension 0): one contiguous span [x, y) of the cell-ordered points,
+// because the non-empty cells are sorted by linear id.
+__device__ __forceinline__ uint2 cell_span(const HjCellHash& h, const uint32_t* cell_start, unsigned long long lo,
+                                           uint32_t w) {
+    uint32_t first = kNoCell, last = kNoCell;
+    for (uint32_t i = 0; i < w; ++i) {
+        const uint32_t c = cell_find(h, lo + i);
+        if (c != kNoCell) {
+            if (first == kNoCell) first = c;
+            last = c;
+        }
+    }
+    if (first == kNoCell) return make_uint2(0u, 0u);
+    return make_uint2(cell_start[first], cell_start[last + 1]);
+}
 
 }  // namespace hj

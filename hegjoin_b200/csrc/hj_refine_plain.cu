@@ -37,6 +37,7 @@ struct PlainArgs {
     const unsigned long long* cell_lid;
     const uint32_t* cell_start;
     uint32_t nC;
+    HjCellHash hash;
     uint32_t d;
     HjGrid grid;
     T thr;
@@ -48,14 +49,6 @@ struct PlainArgs {
     unsigned long long* block_counts;   // count-only mode: pairs per work item
 };
 
-__device__ __forceinline__ uint32_t lower_bound_lid(const unsigned long long* a, uint32_t n, unsigned long long v) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (a[mid] < v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
 
 // Packed FP32 pairs (sm_100): each lane's result is the IEEE-rounded scalar
 // operation, so the packed loop is bit-identical to the scalar one.
@@ -89,9 +82,11 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
     T* c_s = q_s + (size_t)d * QB;                              // [d][CB]
     uint32_t* qid_s = reinterpret_cast<uint32_t*>(c_s + (size_t)d * CB);  // [QB]
     uint32_t* cpos_s = qid_s + QB;                              // [CB]
-    uint32_t* rs = cpos_s + CB;                                 // [kRowGroup] range starts
+    uint32_t* cid_s = cpos_s + CB;                              // [CB] original ids of the chunk
+    uint32_t* rs = cid_s + CB;                                  // [kRowGroup] range starts
     uint32_t* rp = rs + kRowGroup;                              // [kRowGroup + 1] prefix of lengths
     __shared__ uint32_t s_item;
+    __shared__ uint32_t wsum_s[17];   // row-group scan: warp totals, their prefixes, the group total
 
     const uint32_t tid = threadIdx.x;
     const uint32_t tx = tid % TX, ty = tid / TX;
@@ -134,45 +129,44 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
             for (uint32_t row0 = 0; row0 < rows; row0 += kRowGroup) {
                 const uint32_t nr = min(kRowGroup, rows - row0);
                 __syncthreads();
-                if (tid < 32) {
-                    // resolve the rows of this group into point ranges, then prefix their lengths
-                    uint32_t lens[kRowGroup / 32];
-                    uint32_t my = 0;
-#pragma unroll
-                    for (uint32_t s = 0; s < kRowGroup / 32; ++s) {
-                        uint32_t r = tid * (kRowGroup / 32) + s;
-                        uint32_t len = 0, st = 0;
-                        if (r < nr) {
-                            uint32_t rem = row0 + r;
-                            unsigned long long base = 0;
-                            for (uint32_t j = 1; j < k; ++j) {
-                                uint32_t t = lo[j] + rem % w[j];
-                                rem /= w[j];
-                                base += (unsigned long long)t * a.grid.mult[j];
-                            }
-                            unsigned long long la = base + lo[0], lb = la + w[0] - 1;
-                            uint32_t c0 = lower_bound_lid(a.cell_lid, a.nC, la), c1 = c0;
-                            while (c1 < a.nC && a.cell_lid[c1] <= lb) ++c1;
-                            st = a.cell_start[c0];
-                            len = a.cell_start[c1] - st;
-                            rs[r] = st;
+                {
+                    // every thread resolves one row of this group into a point range (through
+                    // the cell hash), then the block prefixes the lengths: warp scans, then a
+                    // scan of the 8 warp totals
+                    uint32_t len = 0;
+                    if (tid < nr) {
+                        uint32_t rem = row0 + tid;
+                        unsigned long long base = 0;
+                        for (uint32_t j = 1; j < k; ++j) {
+                            uint32_t t = lo[j] + rem % w[j];
+                            rem /= w[j];
+                            base += (unsigned long long)t * a.grid.mult[j];
                         }
-                        lens[s] = len;
-                        my += len;
+                        const uint2 sp = cell_span(a.hash, a.cell_start, base + lo[0], w[0]);
+                        rs[tid] = sp.x;
+                        len = sp.y - sp.x;
                     }
-                    uint32_t incl = my;
+                    uint32_t incl = len;
+#pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
                         uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (tid >= (uint32_t)o) incl += t;
+                        if (lane_id() >= (uint32_t)o) incl += t;
                     }
-                    uint32_t run = incl - my;
+                    if (lane_id() == 31) wsum_s[tid >> 5] = incl;
+                    __syncthreads();
+                    if (tid < 32) {
+                        uint32_t v = tid < 8 ? wsum_s[tid] : 0u, x = v;
 #pragma unroll
-                    for (uint32_t s = 0; s < kRowGroup / 32; ++s) {
-                        uint32_t r = tid * (kRowGroup / 32) + s;
-                        if (r < nr) rp[r] = run;
-                        run += lens[s];
+                        for (int o = 1; o < 8; o <<= 1) {
+                            uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+                            if (tid >= (uint32_t)o) x += t;
+                        }
+                        if (tid < 8) wsum_s[8 + tid] = x - v;   // exclusive warp offsets
+                        if (tid == 7) wsum_s[16] = x;           // group total
                     }
-                    if (tid == 31) rp[nr] = incl;
+                    __syncthreads();
+                    if (tid < nr) rp[tid] = wsum_s[8 + (tid >> 5)] + incl - len;
+                    if (tid == 0) rp[nr] = wsum_s[16];
                 }
                 __syncthreads();
                 const uint32_t total = rp[nr];
@@ -188,6 +182,8 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
                             p = rs[lo2] + (v - rp[lo2]);
                         }
                         cpos_s[j] = p;
+                        // staged once per chunk, so emitting a pair reads shared memory only
+                        if (!a.count_only) cid_s[j] = p != kNoPos ? a.perm[p] : 0u;
                     }
                     __syncthreads();
                     for (uint32_t f = tid; f < (uint32_t)CB * d; f += 256) {
@@ -263,12 +259,12 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
                     if (a.count_only) {
                         item_cnt += __popc(mask);
                     } else {
-                        uint32_t m = mask;
-                        warp_emit(a.sink, wc, __popc(mask), [&](uint32_t) {
-                            uint32_t b = __ffs(m) - 1;
-                            m &= m - 1;
-                            uint32_t qi = ty * RQ + b / RC, cj = tx * RC + b % RC;
-                            return make_uint2(qid_s[qi], a.perm[cpos_s[cj]]);
+                        // coalesced output: each lane writes every 32nd pair of the warp's hits
+                        const uint32_t wbase = tid & ~31u;
+                        warp_emit_masks(a.sink, wc, mask, [&](uint32_t owner, uint32_t b) {
+                            const uint32_t ot = wbase + owner;
+                            const uint32_t qi = (ot / TX) * RQ + b / RC, cj = (ot % TX) * RC + b % RC;
+                            return make_uint2(qid_s[qi], cid_s[cj]);
                         });
                     }
                     __syncthreads();
@@ -286,7 +282,7 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
 
 template <typename T, int D, int QB, int CB, int RQ, int RC>
 hj_status launch_t(const PlainArgs<T>& args, cudaStream_t st) {
-    size_t smem = (size_t)(D ? D : args.d) * (QB + CB) * sizeof(T) + (QB + CB + 2 * kRowGroup + 1) * sizeof(uint32_t);
+    size_t smem = (size_t)(D ? D : args.d) * (QB + CB) * sizeof(T) + (QB + 2 * CB + 2 * kRowGroup + 1) * sizeof(uint32_t);
     auto kern = k_refine_plain<T, D, QB, CB, RQ, RC>;
     HJ_TRY(ensure_smem(kern, smem));
     int per_sm = 0;
@@ -337,11 +333,13 @@ hj_status launch_refine_plain(const hj_index* ix, const HjBlock* blocks, uint32_
                               cudaStream_t st) {
     if (nblocks == 0) return HJ_OK;
     if (ix->dtype == HJ_F32) {
-        PlainArgs<float> a{(const float*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, ix->d, ix->grid,
+        PlainArgs<float> a{(const float*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, cell_hash(ix), ix->d,
+                           ix->grid,
                            (float)ix->thr, blocks, nblocks, head, sink, count_only, block_counts};
         return dispatch_t<float>(a, st);
     }
-    PlainArgs<double> a{(const double*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, ix->d, ix->grid,
+    PlainArgs<double> a{(const double*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, cell_hash(ix), ix->d,
+                        ix->grid,
                         ix->thr, blocks, nblocks, head, sink, count_only, block_counts};
     return dispatch_t<double>(a, st);
 }

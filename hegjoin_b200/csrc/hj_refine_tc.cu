@@ -70,6 +70,7 @@ struct TcArgs {
     const unsigned long long* cell_lid;
     const uint32_t* cell_start;
     uint32_t nC;
+    HjCellHash hash;
     HjGrid grid;
     const float4* pinfo;        // per sorted point: quantisation error norm, |x~|^2, norm-split residual
     uint32_t n;
@@ -105,14 +106,6 @@ struct TcShared {
     uint32_t tp[kMaxRanges + 1];           // tile prefix
 };
 
-__device__ __forceinline__ uint32_t lower_bound_lid(const unsigned long long* a, uint32_t n, unsigned long long v) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (a[mid] < v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
 
 // Tiles are visited in order, so the range of tile t is found by walking r
 // forward from the previous tile's range (the last r with tp[r] <= t; ranges
@@ -280,11 +273,9 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                         rem /= w[j];
                         bse += (unsigned long long)t * a.grid.mult[j];
                     }
-                    unsigned long long la = bse + lo[0], lb = la + w[0] - 1;
-                    uint32_t c0 = lower_bound_lid(a.cell_lid, a.nC, la), c1 = c0;
-                    while (c1 < a.nC && a.cell_lid[c1] <= lb) ++c1;
-                    st = a.cell_start[c0];
-                    len = a.cell_start[c1] - st;
+                    const uint2 sp = cell_span(a.hash, a.cell_start, bse + lo[0], w[0]);
+                    st = sp.x;
+                    len = sp.y - sp.x;
                     S.rs[r] = st;
                     S.rl[r] = len;
                 }
@@ -876,6 +867,7 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     TcArgs a{};
     a.blocks = blocks; a.nblocks = nblocks; a.head = head;
     a.perm = ix->perm; a.cell_lid = ix->cell_lid; a.cell_start = ix->cell_start; a.nC = ix->nC; a.grid = ix->grid;
+    a.hash = cell_hash(ix);
     a.pinfo = reinterpret_cast<const float4*>(ix->tc_err);
     a.n = ix->n; a.nkb = nkb; a.stages = stages;
     a.thr = (float)ix->thr;
