@@ -231,9 +231,9 @@ __global__ void k_cell_workload(const unsigned long long* __restrict__ cell_lid,
     uint32_t lo[kMaxK], w[kMaxK];
     uint32_t rows = 1;
     bool empty = false;
+    const uint32_t cl = lane_cell_coord(grid, L);
     for (uint32_t j = 0; j < grid.k; ++j) {
-        uint32_t c = (uint32_t)((L / grid.mult[j]) % grid.n_cells[j]);
-        if (j == grid.k - 1) c = (uint32_t)(L / grid.mult[j]);
+        const uint32_t c = __shfl_sync(0xffffffffu, cl, j);
         uint32_t l = c - 1u;                                   // wraps at 0 (kernel.cu:113)
         uint32_t h = min(grid.n_cells[j] - 1u, c + 1u);        // kernel.cu:114
         if (l > h) empty = true;
@@ -247,8 +247,9 @@ __global__ void k_cell_workload(const unsigned long long* __restrict__ cell_lid,
             uint32_t rem = r;
             unsigned long long base = 0;
             for (uint32_t j = 1; j < grid.k; ++j) {
-                uint32_t t = lo[j] + rem % w[j];
-                rem /= w[j];
+                const uint32_t qw = div_w(rem, w[j]);
+                uint32_t t = lo[j] + (rem - qw * w[j]);
+                rem = qw;
                 base += (unsigned long long)t * grid.mult[j];
             }
             const uint2 sp = cell_span(hash, cell_start, base + lo[0], w[0]);

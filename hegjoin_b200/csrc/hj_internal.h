@@ -87,6 +87,22 @@ constexpr uint32_t kNoCell = 0xFFFFFFFFu;
 
 inline HjCellHash cell_hash(const hj_index* ix) { return HjCellHash{ix->hash_keys, ix->hash_vals, ix->hash_mask}; }
 
+// Coordinate of the cell with linear id L along dimension lane_id() for the
+// lanes below k: the warp pays one 64-bit division per lane, and the other
+// dimensions are fetched with shuffles, instead of k divisions per thread.
+__device__ __forceinline__ uint32_t lane_cell_coord(const HjGrid& g, unsigned long long L) {
+    const uint32_t j = lane_id();
+    if (j >= g.k) return 0u;
+    const unsigned long long q = L / g.mult[j];
+    return (j + 1 < g.k) ? (uint32_t)(q % g.n_cells[j]) : (uint32_t)q;
+}
+
+// Quotient of r by a stencil width w in {1, 2, 3} (widths are 3 except where
+// the stencil is clamped at the grid's edge): no integer division instruction.
+__device__ __forceinline__ uint32_t div_w(uint32_t r, uint32_t w) {
+    return w == 3u ? (uint32_t)(((unsigned long long)r * 0xAAAAAAABull) >> 33) : (w == 2u ? r >> 1 : r);
+}
+
 // Cell index of linear id `lid`, or kNoCell.  Probes stop at a free slot; the
 // table is at most half full, so the loop ends after a few probes (and after
 // capacity probes at the very most).

@@ -71,8 +71,104 @@ __device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double ffma(double a, double b, double c) { return __fma_rn(a, b, c); }
 
+// Warp path for small work items: one warp joins one item on its own, with no
+// block-wide barrier.  The item's queries (at most 32 / D of them per pass) sit
+// in lane registers and are broadcast with shuffles; every lane resolves its
+// own stencil rows through the cell hash (RPL rows per round) and walks their
+// candidates, the warp stepping together through the longest row of the round.
+// Used once the workload order reaches items with nq * D <= 32 and at most
+// 4096 candidate pairs, when k >= 4 (3^(k-1) >= 27 stencil rows per item):
+// there the block path's barriers and staging cost more than the pairs.
+template <typename T, int D>
+__device__ __forceinline__ void warp_item(const PlainArgs<T>& a, const HjBlock& blk, WarpChunk& wc, uint32_t* wsm,
+                                          unsigned long long& item_cnt) {
+    constexpr uint32_t G = 32u / D;      // queries per pass
+    constexpr uint32_t RPL = 4;          // stencil rows per lane per round
+    const uint32_t lane = lane_id();
+    const uint32_t k = a.grid.k;
+    const uint32_t nq = blk.q1 - blk.q0;
+    const unsigned long long L = a.cell_lid[blk.cell];
+    uint32_t lo[kMaxK], w[kMaxK];
+    uint32_t rows = 1;
+    bool empty = false;
+    const uint32_t cl = lane_cell_coord(a.grid, L);
+    for (uint32_t j = 0; j < k; ++j) {
+        const uint32_t c = __shfl_sync(0xffffffffu, cl, j);
+        uint32_t l = c - 1u;                                // kernel.cu:780, wraps at 0
+        uint32_t h = min(a.grid.n_cells[j] - 1u, c + 1u);   // kernel.cu:781
+        empty |= l > h;
+        lo[j] = l;
+        w[j] = h - l + 1u;
+        if (j > 0) rows *= w[j];
+    }
+    if (empty) return;
+    uint32_t* cid_w = wsm;        // [32] candidate ids of the current step
+    uint32_t* qid_w = wsm + 32;   // [32] original ids of the current pass's queries
+    for (uint32_t qg = 0; qg < nq; qg += G) {
+        const uint32_t gq = min(G, nq - qg);
+        // lane L holds coordinate L % D of query qg + L / D
+        const T qv = lane < gq * D ? a.pts[(size_t)(blk.q0 + qg + lane / D) * D + lane % D] : T(0);
+        if (!a.count_only) qid_w[lane] = lane < gq ? a.perm[blk.q0 + qg + lane] : 0u;
+        __syncwarp();
+        for (uint32_t rb = 0; rb < rows; rb += 32 * RPL) {
+            uint32_t st[RPL], len[RPL];
+#pragma unroll
+            for (uint32_t sl = 0; sl < RPL; ++sl) {
+                const uint32_t r = rb + sl * 32 + lane;
+                st[sl] = 0;
+                len[sl] = 0;
+                if (r < rows) {
+                    uint32_t rem = r;
+                    unsigned long long base = 0;
+                    for (uint32_t j = 1; j < k; ++j) {
+                        const uint32_t qw = div_w(rem, w[j]);
+                        base += (unsigned long long)(lo[j] + (rem - qw * w[j])) * a.grid.mult[j];
+                        rem = qw;
+                    }
+                    const uint2 sp = cell_span(a.hash, a.cell_start, base + lo[0], w[0]);
+                    st[sl] = sp.x;
+                    len[sl] = sp.y - sp.x;
+                }
+            }
+#pragma unroll
+            for (uint32_t sl = 0; sl < RPL; ++sl) {
+                const uint32_t steps = __reduce_max_sync(0xffffffffu, len[sl]);
+                for (uint32_t jj = 0; jj < steps; ++jj) {
+                    const bool valid = jj < len[sl];
+                    const uint32_t p = st[sl] + jj;
+                    T cv[D];
+#pragma unroll
+                    for (int l = 0; l < D; ++l) cv[l] = valid ? a.pts[(size_t)p * D + l] : T(0);
+                    uint32_t mask = 0;
+#pragma unroll
+                    for (uint32_t qi = 0; qi < G; ++qi) {
+                        T acc = T(0);
+#pragma unroll
+                        for (int l = 0; l < D; ++l) {
+                            const T q = __shfl_sync(0xffffffffu, qv, qi * D + l);
+                            const T diff = fsub(cv[l], q);   // candidate - query (kernel.cu:351)
+                            acc = ffma(diff, diff, acc);
+                        }
+                        mask |= (uint32_t)(valid && qi < gq && acc <= a.thr) << qi;
+                    }
+                    if (a.count_only) {
+                        item_cnt += __popc(mask);
+                    } else {
+                        cid_w[lane] = valid ? a.perm[p] : 0u;
+                        __syncwarp();
+                        warp_emit_masks(a.sink, wc, mask,
+                                        [&](uint32_t owner, uint32_t b) { return make_uint2(qid_w[b], cid_w[owner]); });
+                        __syncwarp();
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 template <typename T, int D, int QB, int CB, int RQ, int RC>
-__global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
+__global__ void __launch_bounds__(256, 3) k_refine_plain(PlainArgs<T> a) {
     static_assert((QB / RQ) * (CB / RC) == 256, "tile must map onto 256 threads");
     static_assert(RQ * RC <= 32, "hit mask is 32 bits");
     constexpr int TX = CB / RC;
@@ -87,6 +183,8 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
     uint32_t* rp = rs + kRowGroup;                              // [kRowGroup + 1] prefix of lengths
     __shared__ uint32_t s_item;
     __shared__ uint32_t wsum_s[17];   // row-group scan: warp totals, their prefixes, the group total
+    __shared__ uint32_t warp_sm[8][64];   // warp path: candidate and query ids per warp
+    constexpr bool kWarpPath = D != 0 && D <= 32;
 
     const uint32_t tid = threadIdx.x;
     const uint32_t tx = tid % TX, ty = tid / TX;
@@ -102,6 +200,33 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
         const HjBlock blk = a.blocks[item];
         const uint32_t nq = blk.q1 - blk.q0;
 
+        if constexpr (kWarpPath) {
+            // from the first item whose queries fit the warp path, every warp of the block
+            // takes items on its own until the order is exhausted (the decision is
+            // block-uniform: all threads read the same item)
+            if (k >= 4u && nq * (uint32_t)D <= 32u && (unsigned long long)blk.nb * nq <= 4096ull) {
+                const uint32_t wid = tid >> 5;
+                uint32_t it_w = item;   // warp 0 takes the item already fetched
+                if (wid != 0) {
+                    uint32_t nx = 0;
+                    if (lane_id() == 0) nx = atomicAdd(a.head, 1u);
+                    it_w = __shfl_sync(0xffffffffu, nx, 0);
+                }
+                while (it_w < a.nblocks) {
+                    unsigned long long cnt_w = 0;
+                    warp_item<T, D>(a, a.blocks[it_w], wc, warp_sm[wid], cnt_w);
+                    if (a.count_only) {
+                        for (int o = 16; o > 0; o >>= 1) cnt_w += __shfl_down_sync(0xffffffffu, cnt_w, o);
+                        if (lane_id() == 0 && cnt_w) atomicAdd(&a.block_counts[it_w], cnt_w);
+                    }
+                    uint32_t nx = 0;
+                    if (lane_id() == 0) nx = atomicAdd(a.head, 1u);
+                    it_w = __shfl_sync(0xffffffffu, nx, 0);
+                }
+                break;
+            }
+        }
+
         // queries, dimension-major
         for (uint32_t f = tid; f < (uint32_t)QB * d; f += 256) {
             uint32_t i = f / d, l = f - i * d;
@@ -114,9 +239,9 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
         uint32_t lo[kMaxK], w[kMaxK];
         uint32_t rows = 1;
         bool empty = false;
+        const uint32_t cl = lane_cell_coord(a.grid, L);
         for (uint32_t j = 0; j < k; ++j) {
-            uint32_t c = (j + 1 < k) ? (uint32_t)((L / a.grid.mult[j]) % a.grid.n_cells[j])
-                                     : (uint32_t)(L / a.grid.mult[j]);
+            const uint32_t c = __shfl_sync(0xffffffffu, cl, j);
             uint32_t l = c - 1u;                                // kernel.cu:780, wraps at 0
             uint32_t h = min(a.grid.n_cells[j] - 1u, c + 1u);   // kernel.cu:781
             empty |= l > h;
@@ -138,8 +263,9 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
                         uint32_t rem = row0 + tid;
                         unsigned long long base = 0;
                         for (uint32_t j = 1; j < k; ++j) {
-                            uint32_t t = lo[j] + rem % w[j];
-                            rem /= w[j];
+                            const uint32_t qw = div_w(rem, w[j]);
+                            uint32_t t = lo[j] + (rem - qw * w[j]);
+                            rem = qw;
                             base += (unsigned long long)t * a.grid.mult[j];
                         }
                         const uint2 sp = cell_span(a.hash, a.cell_start, base + lo[0], w[0]);
@@ -193,9 +319,17 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
                     }
                     __syncthreads();
                     const uint32_t nvalid = min((uint32_t)CB, total - cb);
+                    // threads whose whole tile lies past the queries or the candidates skip the
+                    // arithmetic (small work items: one query against a few candidates)
+                    const bool live = ty * RQ < nq && tx * RC < nvalid;
 
                     T acc[RQ][RC];
-                    if constexpr (std::is_same<T, float>::value && RC % 2 == 0) {
+                    if (!live) {
+#pragma unroll
+                        for (int r = 0; r < RQ; ++r)
+#pragma unroll
+                            for (int c = 0; c < RC; ++c) acc[r][c] = T(0);
+                    } else if constexpr (std::is_same<T, float>::value && RC % 2 == 0) {
                         // candidate pairs (c, c+1) packed: diff = c - q, acc = fma(diff, diff, acc)
                         unsigned long long acc2[RQ][RC / 2];
 #pragma unroll
@@ -253,7 +387,7 @@ __global__ void __launch_bounds__(256) k_refine_plain(PlainArgs<T> a) {
                     for (int r = 0; r < RQ; ++r)
 #pragma unroll
                         for (int c = 0; c < RC; ++c) {
-                            bool hit = acc[r][c] <= a.thr && (ty * RQ + r) < nq && (tx * RC + c) < nvalid;
+                            bool hit = live && acc[r][c] <= a.thr && (ty * RQ + r) < nq && (tx * RC + c) < nvalid;
                             mask |= (hit ? 1u : 0u) << (r * RC + c);
                         }
                     if (a.count_only) {

@@ -101,6 +101,7 @@ struct TcShared {
     uint32_t nq, nqt, ntiles, nr, q0;
     uint32_t max_e, max_n, max_r;          // float bits (non-negative)
     uint32_t qid[kQB];
+    uint32_t cidw[16 * 32];                // epilogue warp w, lane l: original id of its current row
     uint32_t rs[kMaxRanges];               // range start (sorted position)
     uint32_t rl[kMaxRanges];               // range length
     uint32_t tp[kMaxRanges + 1];           // tile prefix
@@ -248,9 +249,9 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
             uint32_t lo[kMaxK], w[kMaxK];
             uint32_t rows = 1;
             bool empty = false;
+            const uint32_t cl = lane_cell_coord(a.grid, L);
             for (uint32_t j = 0; j < k; ++j) {
-                uint32_t c = (j + 1 < k) ? (uint32_t)((L / a.grid.mult[j]) % a.grid.n_cells[j])
-                                         : (uint32_t)(L / a.grid.mult[j]);
+                const uint32_t c = __shfl_sync(0xffffffffu, cl, j);
                 uint32_t l = c - 1u;                                // kernel.cu:780, wraps at 0
                 uint32_t h = min(a.grid.n_cells[j] - 1u, c + 1u);   // kernel.cu:781
                 empty |= l > h;
@@ -269,8 +270,9 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                     uint32_t rem = r;
                     unsigned long long bse = 0;
                     for (uint32_t j = 1; j < k; ++j) {
-                        uint32_t t = lo[j] + rem % w[j];
-                        rem /= w[j];
+                        const uint32_t qw = div_w(rem, w[j]);
+                        uint32_t t = lo[j] + (rem - qw * w[j]);
+                        rem = qw;
                         bse += (unsigned long long)t * a.grid.mult[j];
                     }
                     const uint2 sp = cell_span(a.hash, a.cell_start, bse + lo[0], w[0]);
@@ -429,6 +431,8 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                     tw.locate(S, t + 1);
                 }
                 const uint32_t cid = cid_next;
+                S.cidw[ew * 32 + lane] = cid;   // read by the lanes that write this row's pairs
+                __syncwarp();
                 if (t + 1 < ntiles && row < tw.valid) {
                     pc = a.pinfo[tw.start + row];
                     if (!a.count_only) cid_next = a.perm[tw.start + row];
@@ -481,19 +485,16 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                                 n_acc += __popc(amask);
                                 n_band += __popc(bmask);
                                 if (a.count_only) continue;
+                                // coalesced output: each lane writes every 32nd pair of the warp's
+                                // hits; the owner lane's row gives the candidate
                                 const uint32_t qcol = j * kAccCols + cbase;
-                                uint32_t m1 = amask;
-                                warp_emit(a.sink, wc_acc, __popc(amask), [&](uint32_t) {
-                                    uint32_t b = __ffs(m1) - 1;
-                                    m1 &= m1 - 1;
-                                    return make_uint2(S.qid[qcol + b], cid);
+                                const uint32_t* cidw = &S.cidw[ew * 32];
+                                warp_emit_masks(a.sink, wc_acc, amask, [&](uint32_t owner, uint32_t b) {
+                                    return make_uint2(S.qid[qcol + b], cidw[owner]);
                                 });
-                                uint32_t m2 = bmask;
-                                const uint32_t q0 = S.q0;
-                                warp_emit(a.band, wc_band, __popc(bmask), [&](uint32_t) {
-                                    uint32_t b = __ffs(m2) - 1;
-                                    m2 &= m2 - 1;
-                                    return make_uint2(q0 + qcol + b, cpos);
+                                const uint32_t q0 = S.q0, cpos0 = cpos - lane;
+                                warp_emit_masks(a.band, wc_band, bmask, [&](uint32_t owner, uint32_t b) {
+                                    return make_uint2(q0 + qcol + b, cpos0 + owner);
                                 });
                             }
                         }
