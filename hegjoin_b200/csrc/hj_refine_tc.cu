@@ -163,7 +163,10 @@ __device__ __forceinline__ float minN(const float (&v)[N]) {
 // the epilogue warps form one set per accumulator (a warp drains half as many
 // accumulators, each over a whole tile's MMA time) instead of every warp draining
 // both.  Which is faster depends on d: the autotuner times all four shapes.
-template <int EPI, bool SPLIT>
+// DEFER: one vote per accumulator instead of one per chunk, chunks with a hit
+// read again before the release; it pays where hits are rare (picked from the
+// estimated pair density).
+template <int EPI, bool SPLIT, bool DEFER>
 __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     k_refine_tc(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query, TcArgs a) {
     static_assert(EPI == 2 || EPI == 4, "an epilogue set needs whole groups of 4 warps");
@@ -398,9 +401,9 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
             uint32_t n_acc = 0, n_band = 0;
             bool ok = true;
             // this warp's columns of an accumulator: COLS = 256 / (SETW / 4), read in chunks
-            // of LDW by tcgen05.ld, W chunks per wait ("wave"); the accumulator is handed back
-            // once the last wave is in registers.  EPI 4 leaves 96 registers a thread: two
-            // 32-column chunks per wave when a warp has 64 columns, one when it has 128.
+            // of LDW by tcgen05.ld, W chunks per wait ("wave").  EPI 4 leaves 96 registers a
+            // thread: two 32-column chunks per wave when a warp has 64 columns, one when it
+            // has 128.
             constexpr uint32_t COLS = kAccCols / (SETW / 4);
             constexpr uint32_t LDW = EPI == 4 ? 32u : 64u;
             constexpr uint32_t NCH = COLS / LDW;
@@ -445,40 +448,45 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                     }
                     tc::fence_after();
                     const uint32_t ncols = min((uint32_t)kAccCols, nq - j * kAccCols);
-#pragma unroll 1
-                    for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
-                        float v[W][LDW];
-#pragma unroll
-                        for (uint32_t w = 0; w < W; ++w) {
-                            const uint32_t col = grp * COLS + (c0 + w) * LDW;
-                            if constexpr (LDW == 64) {
-                                tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v[w]);
-                            } else {
-                                tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v[w]);
-                            }
+                    if constexpr (DEFER) {
+                        // fast pass: min-reduce every chunk and note, per row, the chunks with a value
+                        // at or below the upper band edge; no vote or branch per chunk
+                        uint32_t hitw = 0;
+                        auto load_chunk = [&](float (&v)[LDW], uint32_t c) {
+                            const uint32_t col = grp * COLS + c * LDW;
+                            if constexpr (LDW == 64) tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v);
+                            else tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v);
+                        };
+    #pragma unroll 1
+                        for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
+                            float v[W][LDW];
+    #pragma unroll
+                            for (uint32_t w = 0; w < W; ++w) load_chunk(v[w], c0 + w);
+                            tc::tmem_ld_wait();
+    #pragma unroll
+                            for (uint32_t w = 0; w < W; ++w) hitw |= (uint32_t)(minN<LDW>(v[w]) <= hi) << (c0 + w);
                         }
-                        tc::tmem_ld_wait();
-                        if (c0 + W >= NCH) {
-                            // all of this warp's columns are in registers: release the accumulator
-                            tc::fence_before();
-                            __syncwarp();
-                            if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
-                        }
-#pragma unroll
-                        for (uint32_t w = 0; w < W; ++w) {
-                            const uint32_t col0 = grp * COLS + (c0 + w) * LDW;
-                            const bool any_hit = minN<LDW>(v[w]) <= hi;
-                            if (!__any_sync(0xffffffffu, any_hit)) continue;
-#pragma unroll
+                        // chunks where some row hit are read again (rare: the accumulator is still
+                        // held) and classified pair by pair
+                        uint32_t wave_hits = __reduce_or_sync(0xffffffffu, hitw);
+                        while (wave_hits) {
+                            const uint32_t c = __ffs(wave_hits) - 1;
+                            wave_hits &= wave_hits - 1;
+                            float v[LDW];
+                            load_chunk(v, c);
+                            tc::tmem_ld_wait();
+                            const bool any_hit = (hitw >> c) & 1u;
+                            const uint32_t col0 = grp * COLS + c * LDW;
+    #pragma unroll
                             for (uint32_t h = 0; h < LDW / 32; ++h) {
                                 const uint32_t cbase = col0 + h * 32u;
                                 uint32_t hmask = 0, amask = 0;
                                 if (any_hit) {
-#pragma unroll
+    #pragma unroll
                                     for (int i = 0; i < 32; ++i) {
                                         bool inq = cbase + i < ncols;
-                                        hmask |= (uint32_t)(inq && v[w][h * 32 + i] <= hi) << i;
-                                        amask |= (uint32_t)(inq && v[w][h * 32 + i] <= lo) << i;
+                                        hmask |= (uint32_t)(inq && v[h * 32 + i] <= hi) << i;
+                                        amask |= (uint32_t)(inq && v[h * 32 + i] <= lo) << i;
                                     }
                                 }
                                 const uint32_t bmask = hmask & ~amask;
@@ -496,6 +504,67 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                                 warp_emit_masks(a.band, wc_band, bmask, [&](uint32_t owner, uint32_t b) {
                                     return make_uint2(q0 + qcol + b, cpos0 + owner);
                                 });
+                            }
+                        }
+                        // every column of this warp has been read: release the accumulator
+                        tc::fence_before();
+                        __syncwarp();
+                        if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
+                    } else {
+                        // per chunk: min-reduce, vote, and classify at once; the accumulator is
+                        // released as soon as the last wave is in registers
+    #pragma unroll 1
+                        for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
+                            float v[W][LDW];
+    #pragma unroll
+                            for (uint32_t w = 0; w < W; ++w) {
+                                const uint32_t col = grp * COLS + (c0 + w) * LDW;
+                                if constexpr (LDW == 64) {
+                                    tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v[w]);
+                                } else {
+                                    tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v[w]);
+                                }
+                            }
+                            tc::tmem_ld_wait();
+                            if (c0 + W >= NCH) {
+                                // all of this warp's columns are in registers: release the accumulator
+                                tc::fence_before();
+                                __syncwarp();
+                                if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
+                            }
+    #pragma unroll
+                            for (uint32_t w = 0; w < W; ++w) {
+                                const uint32_t col0 = grp * COLS + (c0 + w) * LDW;
+                                const bool any_hit = minN<LDW>(v[w]) <= hi;
+                                if (!__any_sync(0xffffffffu, any_hit)) continue;
+    #pragma unroll
+                                for (uint32_t h = 0; h < LDW / 32; ++h) {
+                                    const uint32_t cbase = col0 + h * 32u;
+                                    uint32_t hmask = 0, amask = 0;
+                                    if (any_hit) {
+    #pragma unroll
+                                        for (int i = 0; i < 32; ++i) {
+                                            bool inq = cbase + i < ncols;
+                                            hmask |= (uint32_t)(inq && v[w][h * 32 + i] <= hi) << i;
+                                            amask |= (uint32_t)(inq && v[w][h * 32 + i] <= lo) << i;
+                                        }
+                                    }
+                                    const uint32_t bmask = hmask & ~amask;
+                                    n_acc += __popc(amask);
+                                    n_band += __popc(bmask);
+                                    if (a.count_only) continue;
+                                    // coalesced output: each lane writes every 32nd pair of the warp's
+                                    // hits; the owner lane's row gives the candidate
+                                    const uint32_t qcol = j * kAccCols + cbase;
+                                    const uint32_t* cidw = &S.cidw[ew * 32];
+                                    warp_emit_masks(a.sink, wc_acc, amask, [&](uint32_t owner, uint32_t b) {
+                                        return make_uint2(S.qid[qcol + b], cidw[owner]);
+                                    });
+                                    const uint32_t q0 = S.q0, cpos0 = cpos - lane;
+                                    warp_emit_masks(a.band, wc_band, bmask, [&](uint32_t owner, uint32_t b) {
+                                        return make_uint2(q0 + qcol + b, cpos0 + owner);
+                                    });
+                                }
                             }
                         }
                     }
@@ -755,6 +824,7 @@ struct TcMaps {
 struct TcState {
     TcMaps maps;
     int epi = 4;              // epilogue shape code, EPI | 8 * SPLIT (autotuned: 2, 4, 10, 12)
+    bool defer = false;       // one vote per accumulator (set from the estimated pair density)
     float gamma_acc = 0;
     float max_e = 0, max_n = 0, max_r = 0;
 };
@@ -844,6 +914,11 @@ void tc_set_epi(hj_index* ix, int epi) {
     if (s && (epi == 2 || epi == 4 || epi == 10 || epi == 12)) s->epi = epi;
 }
 
+void tc_set_defer(hj_index* ix, bool defer) {
+    TcState* s = tc_state(ix);
+    if (s) s->defer = defer;
+}
+
 void tc_release(hj_index* ix) {
     delete tc_state(ix);
     ix->tc_state = nullptr;
@@ -861,8 +936,14 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     // one CTA per SM: ask for more than half of the SM's shared memory
     smem = std::max<size_t>(smem, 116 * 1024);
     const int code = s->epi;
-    auto kern = code == 2 ? k_refine_tc<2, false>
-                          : code == 10 ? k_refine_tc<2, true> : code == 12 ? k_refine_tc<4, true> : k_refine_tc<4, false>;
+    auto kern = s->defer ? (code == 2    ? k_refine_tc<2, false, true>
+                            : code == 10 ? k_refine_tc<2, true, true>
+                            : code == 12 ? k_refine_tc<4, true, true>
+                                         : k_refine_tc<4, false, true>)
+                         : (code == 2    ? k_refine_tc<2, false, false>
+                            : code == 10 ? k_refine_tc<2, true, false>
+                            : code == 12 ? k_refine_tc<4, true, false>
+                                         : k_refine_tc<4, false, false>);
     const int epi = (code & 7) == 2 ? 2 : 4;
     HJ_TRY(ensure_smem(kern, smem));
     TcArgs a{};

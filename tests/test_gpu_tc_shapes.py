@@ -4,7 +4,8 @@ The autotuner picks one shape per (refine kind, d, dtype) and process, so each
 shape is forced in a child process of its own through a tuning file (the
 library reads "kind d dtype shape" lines from HJ_TUNE_FILE).  Shapes: 2 or 4
 epilogue warp groups, shared by both accumulators (2, 4) or split into one set
-per accumulator (10, 12).
+per accumulator (10, 12); each with one vote per chunk or one per accumulator
+(HJ_TC_DEFER=0/1; the library otherwise picks by the estimated pair density).
 """
 import json
 import os
@@ -40,12 +41,13 @@ CHILD = textwrap.dedent("""
 CASES = [(6000, 18, 6, 0.07), (2500, 90, 6, 0.26), (700, 32, 6, 0.2)]
 
 
+@pytest.mark.parametrize("defer", ["0", "1"])
 @pytest.mark.parametrize("refine,kind", [("tc_f16", 2), ("tc_bf16", 3)])
 @pytest.mark.parametrize("shape", [2, 4, 10, 12])
-def test_shape_matches_oracle(cuda, tmp_path, refine, kind, shape):
+def test_shape_matches_oracle(cuda, tmp_path, refine, kind, shape, defer):
     tune = tmp_path / "tune.txt"
     tune.write_text("".join(f"{kind} {d} 0 {shape}\n" for _, d, _, _ in CASES))
-    env = dict(os.environ, HJ_TUNE_FILE=str(tune))
+    env = dict(os.environ, HJ_TUNE_FILE=str(tune), HJ_TC_DEFER=defer)
     code = CHILD.format(root=ROOT, cases=CASES, refine=refine)
     p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=600)
     assert p.returncode == 0, p.stderr[-3000:]
