@@ -97,7 +97,7 @@ typedef struct {
     double mem_fraction;           /* share of free device memory result buffers may use; 0 = 0.6 */
     uint32_t query_block;          /* queries per work item; 0 = autotuned/default */
     uint32_t max_batches;          /* safety cap on batch count; 0 = unlimited */
-    uint32_t use_graphs;           /* replay the per-batch sequence through a CUDA graph */
+    uint32_t use_graphs;           /* reserved, ignored: a batch is a handful of launches */
     uint32_t keep_keys;            /* keep per-batch sorted key arrays (needed for the reference export) */
     uint32_t shard_count;          /* multi-GPU: work items i with i % shard_count == shard_index (0 = all) */
     uint32_t shard_index;
