@@ -217,6 +217,14 @@ bool tuning_enabled() {
     return !(e && e[0] == '0');
 }
 
+// Tensor-core epilogue: with fewer than ~3% of its 32 x 32 chunks holding a hit, one vote
+// per accumulator and a re-read of the hit chunks beats a vote per chunk (measured at
+// d = 18 with 1.6% and at d = 90 with 6.4%).  HJ_TC_DEFER=0/1 forces either form (tests).
+bool defer_for(double pairs, double cand) {
+    if (const char* e = std::getenv("HJ_TC_DEFER")) return e[0] == '1';
+    return cand > 0 && pairs * 1024.0 < 0.03 * cand;
+}
+
 float ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -383,8 +391,25 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         int tuned = 0;
         const std::string key = tune_key(refine, ix->d, ix->dtype);
         if (tc && !tune_lookup(key, &tuned) && tuning_enabled()) {
-            // time each epilogue width on the sample; the last run's counts are the estimate
-            // epilogue shapes: warp groups | 8 * (one warp set per accumulator)
+            // the vote form follows the hit density: measure it on the sample first, so the
+            // shapes are timed in the form the refine will use
+            HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
+            HJ_TRY(check_timeout());
+            {
+                std::vector<unsigned long long> h0(nsamp);
+                HJ_CUDA(cudaMemcpyAsync(h0.data(), scnt, nsamp * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                        st));
+                HJ_CUDA(cudaStreamSynchronize(st));   // also completes the copy of hblocks
+                double sp = 0, sc = 0;
+                for (uint32_t q = 0; q < nsamp; ++q) {
+                    const HjBlock& b = hblocks[std::min(nblocks - 1, q * stride)];
+                    sp += (double)h0[q];
+                    sc += (double)b.nb * (b.q1 - b.q0);
+                }
+                tc_set_defer(ix, defer_for(sp, sc));
+            }
+            // time each epilogue shape on the sample; the last run's counts are the estimate.
+            // Shapes: warp groups | 8 * (one warp set per accumulator)
             const int cands[4] = {2, 4, 10, 12};
             float best = 1e30f;
             int best_epi = tc_get_epi(ix);
@@ -433,14 +458,9 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     S.estimated_pairs = (uint64_t)total_est;
     S.ms_estimate = ms_since(t_est);
     if (tc) {
-        // Tensor-core epilogue: with fewer than ~3% of its 32 x 32 chunks holding a hit, one
-        // vote per accumulator and a re-read of the hit chunks beats a vote per chunk
-        // (measured at d = 18 with 1.6% and at d = 90 with 6.4%).
         double cand = 0;
         for (uint32_t i = 0; i < nblocks; ++i) cand += (double)hblocks[i].nb * (hblocks[i].q1 - hblocks[i].q0);
-        bool defer = cand > 0 && total_est * 1024.0 < 0.03 * cand;
-        if (const char* e = std::getenv("HJ_TC_DEFER")) defer = e[0] == '1';   // tests force either form
-        tc_set_defer(ix, defer);
+        tc_set_defer(ix, defer_for(total_est, cand));
     }
 
     // ---- result buffer capacity
