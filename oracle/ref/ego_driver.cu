@@ -1,4 +1,4 @@
-// ego_driver.cu -- TEST/BASELINE INFRASTRUCTURE: times the reference's own
+// ego_driver.cu -- TEST AND BENCHMARK INFRASTRUCTURE: times the reference's own
 // CPU join (Super-EGO, the join of algorithm 3) on a bounded query sample.
 //
 // It prepares the points exactly as main.cu does for the Super-EGO thread --
