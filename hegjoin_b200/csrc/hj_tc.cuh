@@ -1,8 +1,8 @@
 // hj_tc.cuh -- inline-PTX wrappers for mbarriers, TMA and tcgen05 (sm_100a).
 //
-// Written from the PTX ISA descriptions of these instructions.  No multicast
-// form is used anywhere: TMA loads are plain tiled loads into this CTA's
-// shared memory and tcgen05.commit signals this CTA's own barriers.
+// Written from the PTX ISA descriptions of these instructions.  TMA loads are
+// plain tiled loads into this CTA's own shared memory, and tcgen05.commit
+// signals this CTA's own barriers.
 #pragma once
 
 #include <cuda.h>
