@@ -171,7 +171,8 @@ hj_status hj_server_create(const hj_server_opts* opts, hj_server** out) {
 
 hj_status hj_server_submit(hj_server* S, const void* h_db, uint32_t n, uint32_t d, uint32_t k, int dtype, double eps,
                            uint64_t* ticket) {
-    if (!S || !h_db || !ticket || n == 0 || d == 0 || k == 0 || k > d) return HJ_ERR_INVALID;
+    if (!S || !h_db || !ticket || n == 0 || d == 0 || k == 0 || k > d || (dtype != HJ_F32 && dtype != HJ_F64))
+        return HJ_ERR_INVALID;
     Req* r = new Req();
     r->h_db = h_db; r->n = n; r->d = d; r->k = k; r->dtype = dtype; r->eps = eps;
     r->reserve = reservation(*r);
