@@ -112,6 +112,7 @@ def _load() -> ctypes.CDLL:
         "hj_self_join_host": (I, [P, U32, U32, U32, I, D, P, P, P, P]),
         "hj_probe_sqdist": (I, [P, P, U32, U32, I, P, P]),
         "hj_probe_tc_tile": (I, [P, I, U32, U32, P, P, P, P]),
+        "hj_tc_operand_scale": (I, [P, P]),
         "hj_shard_plan": (I, [U32, U32, U32, P, P, P]),
         "hj_generate_exp40": (I, [U64, U64, U64, U32, I, P]),
         "hj_generate_skewed": (I, [U64, U64, U32, U32, D, D, I, P]),
@@ -411,8 +412,9 @@ def kpad_for(d: int) -> int:
 def probe_tc_tile(index: GridIndex, refine: str, a0: int, b0: int, stream=None):
     """One candidate tile x 512 queries through the tensor-core path.
 
-    Returns (accumulators [128, 512] float32 numpy, query-form rows [512, kpad],
-    candidate-form rows [128, kpad]) with the operand rows as float64.
+    Returns (accumulators [128, 512], query-form rows [512, kpad], candidate-form
+    rows [128, kpad]) as float64 numpy arrays in the dataset's units: the
+    filter's power-of-two operand scale is divided out exactly.
     """
     torch = _torch()
     inf = index.info()
@@ -422,11 +424,16 @@ def probe_tc_tile(index: GridIndex, refine: str, a0: int, b0: int, stream=None):
     hc = np.zeros((128, kp), np.uint16)
     check(lib.hj_probe_tc_tile(index.handle, REFINE_NAMES[refine], a0, b0, _ptr(out), hq.ctypes.data,
                                hc.ctypes.data, _stream_ptr(stream)))
+    s = ctypes.c_int()
+    check(lib.hj_tc_operand_scale(index.handle, ctypes.byref(s)))
+    # the operand forms hold (x - min) * 2^s: return everything in the dataset's units
+    # (power-of-two scaling is exact)
     if refine == "tc_bf16":
-        conv = lambda a: (a.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+        conv = lambda a: np.ldexp((a.astype(np.uint32) << 16).view(np.float32).astype(np.float64), -s.value)
     else:
-        conv = lambda a: a.view(np.float16).astype(np.float64)
-    return out.cpu().numpy(), conv(hq), conv(hc)
+        conv = lambda a: np.ldexp(a.view(np.float16).astype(np.float64), -s.value)
+    acc = np.ldexp(out.cpu().numpy().astype(np.float64), -2 * s.value)
+    return acc, conv(hq), conv(hc)
 
 
 class Server:

@@ -49,6 +49,21 @@ uint64_t thread_launch_count();   // launches made by the calling thread
         }                                                                               \
     } while (0)
 
+// Status forms of HJ_CUDA / HJ_LAUNCHED for code that must release what it
+// holds before returning (they record the error and return it instead).
+inline hj_status cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return HJ_OK;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? HJ_ERR_OOM : HJ_ERR_CUDA;
+}
+inline hj_status launch_status(const char* file, int line) {
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return HJ_OK;
+    set_error("%s:%d kernel launch: %s", file, line, cudaGetErrorString(e));
+    return e == cudaErrorNoKernelImageForDevice ? HJ_ERR_NO_DEVICE : HJ_ERR_CUDA;
+}
+
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ---- device buffers ----------------------------------------------------------

@@ -47,6 +47,7 @@ hj_status launch_band_recheck(const hj_index* ix, const uint32_t* bq, const uint
                               const unsigned long long* band_used, unsigned long long band_cap,
                               const PairSink& sink, cudaStream_t st);
 double tc_delta(const hj_index* ix);
+double tc_band_ratio(const hj_index* ix);
 bool tc_supported(const hj_index* ix, int kind);
 int tc_get_epi(const hj_index* ix);
 void tc_set_epi(hj_index* ix, int epi);
@@ -294,17 +295,25 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
 
     // ---- refine kind
     int refine = opts.refine;
-    if (refine == HJ_REFINE_AUTO)
+    const bool auto_kind = refine == HJ_REFINE_AUTO;
+    if (auto_kind)
         refine = (ix->dtype == HJ_F32 && ix->d >= 16 && tc_supported(ix, HJ_REFINE_TC_F16)) ? HJ_REFINE_TC_F16
                                                                                             : HJ_REFINE_EXACT;
-    const bool tc = refine == HJ_REFINE_TC_F16 || refine == HJ_REFINE_TC_BF16;
+    bool tc = refine == HJ_REFINE_TC_F16 || refine == HJ_REFINE_TC_BF16;
     if (tc) {
         if (!tc_supported(ix, refine)) {
             set_error("hj_join: the tensor-core filter needs float data with 16 <= d <= %d", 252);
             return HJ_ERR_UNSUPPORTED;
         }
-        HJ_TRY(tc_prepare(ix, refine, st));
-        S.filter_delta = tc_delta(ix);
+        const hj_status ps = tc_prepare(ix, refine, st);
+        if (ps != HJ_OK && !(auto_kind && ps == HJ_ERR_UNSUPPORTED)) return ps;
+        // auto: data the filter cannot take (non-finite coordinates), or whose guard band is
+        // wider than half the threshold (the filter would decide little), go to the exact path
+        if (auto_kind && (ps != HJ_OK || tc_band_ratio(ix) > 0.5)) {
+            refine = HJ_REFINE_EXACT;
+            tc = false;
+        }
+        if (tc) S.filter_delta = tc_delta(ix);
     }
     S.refine_used = (uint32_t)refine;
     uint32_t qb = opts.query_block ? opts.query_block : (tc ? tc_query_block() : plain_query_block(ix->dtype));

@@ -3,23 +3,28 @@
 // hj_grid_geometry keeps its per-block partial minima/maxima in a buffer it
 // allocates for each call.  Some callers cannot allocate device memory at the
 // point where they need the geometry: a process that reserves all of its
-// device memory up front and must never fail on an allocation later, or code
-// running while a CUDA stream is being captured (cudaMalloc is not permitted
-// during capture).  hj_grid_geometry_noalloc serves them: its scratch is the
-// file-scope device array below, so a call allocates nothing.
+// device memory up front (a serving process sized to its HBM budget, or one
+// sharing the GPU under a fixed quota) and must never fail on an allocation
+// later.  hj_grid_geometry_noalloc serves them: its scratch is the file-scope
+// device array below, so a call allocates nothing.  The call copies the
+// reduced minima/maxima to host memory and synchronises its stream, so it
+// cannot run on a stream that is being captured into a CUDA graph.
 //
 // Limits and sharing: the array holds partials for at most kNaBlocks blocks x
-// kNaMaxK indexed dimensions (k <= 16; any n), 151,808 bytes, resident on
-// every GPU that loads the library until the process exits.  All calls on a
-// device share it and it keeps the last call's contents (every slot a call
-// reads is written by that call first), so calls that overlap on the GPU
-// (different streams, or host threads without ordering) race and must be
-// serialised by the caller.  The first call on each device looks up the
-// array's device address (cudaGetSymbolAddress) with that device current; make
-// that first call before any stream capture begins.
+// kNaMaxK indexed dimensions (k <= 16; any n below 2^32), 151,808 bytes,
+// resident on every GPU that loads the library until the process exits.  All
+// calls on a device share it and it keeps the last call's contents (every
+// slot a call reads is written by that call first), so calls that overlap on
+// the GPU (different streams, or host threads without ordering) race and must
+// be serialised by the caller.  The first call on each device looks up the
+// array's device address (cudaGetSymbolAddress) with that device current; the
+// address is looked up again when the device's context has changed since (for
+// example after cudaDeviceReset).
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+
+#include <cuda.h>
 
 #include "hj_internal.h"
 
@@ -35,6 +40,24 @@ static __device__ __align__(256) double g_na_scratch[kNaScratch];
 
 std::mutex g_na_mu;
 double* g_na_addr[64] = {};
+CUcontext g_na_ctx[64] = {};   // the context each cached address belongs to
+
+// cuCtxGetCurrent through the runtime's driver entry-point query (the library
+// does not link libcuda directly).
+CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext*);
+    static Fn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<Fn>(p);
+        return static_cast<Fn>(nullptr);
+    }();
+    CUcontext c = nullptr;
+    if (fn) fn(&c);
+    return c;
+}
 
 template <typename T>
 __global__ void k_na_minmax(const T* __restrict__ db, uint32_t n, uint32_t d, uint32_t k, double* __restrict__ sc) {
@@ -42,8 +65,10 @@ __global__ void k_na_minmax(const T* __restrict__ db, uint32_t n, uint32_t d, ui
     const uint32_t w = threadIdx.x >> 5;
     for (uint32_t j = 0; j < k; ++j) {
         T mn = db[j], mx = db[j];
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-            T v = db[(size_t)i * d + j];
+        // 64-bit index: a 32-bit one would wrap past n near 2^32 and never end the loop
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += (uint64_t)gridDim.x * blockDim.x) {
+            T v = db[i * d + j];
             mn = v < mn ? v : mn;
             mx = v > mx ? v : mx;
         }
@@ -130,8 +155,10 @@ extern "C" hj_status hj_grid_geometry_noalloc(const void* d_db, uint32_t n, uint
     }
     double* sc = nullptr;
     {
+        // the device's current context (cudaGetDevice above made it current)
+        const CUcontext ctx = current_context();
         std::lock_guard<std::mutex> lk(g_na_mu);
-        if (!g_na_addr[dev]) {
+        if (!g_na_addr[dev] || g_na_ctx[dev] != ctx) {
             // first call on this device: the array's device address (host code cannot use its name)
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
@@ -140,6 +167,7 @@ extern "C" hj_status hj_grid_geometry_noalloc(const void* d_db, uint32_t n, uint
                 return e == cudaErrorNoKernelImageForDevice ? HJ_ERR_NO_DEVICE : HJ_ERR_CUDA;
             }
             g_na_addr[dev] = static_cast<double*>(p);
+            g_na_ctx[dev] = ctx;
         }
         sc = g_na_addr[dev];
     }

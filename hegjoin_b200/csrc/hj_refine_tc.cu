@@ -9,16 +9,23 @@
 //   B (N = 2 x 256 queries, resident)       = [  q~, |q~|^2_hi, |q~|^2_lo, 1, 1, 0...]
 //   D = A B^T = |q~|^2 + |c~|^2 - 2 q~.c~ = |q~ - c~|^2        (FP32 accumulate in TMEM)
 //
-// where x~ is the FP16 (or BF16) rounding of x - origin.  The norms ride in the
-// K padding (d + 4 rounded up to 32), so the MMA yields the squared distance
-// directly and the epilogue is one compare per pair.  A pair is
+// where x~ is the FP16 (or BF16) rounding of (x - origin) * 2^s.  The origin
+// is the per-dimension minimum and s is a power-of-two scale chosen per
+// dataset so that the largest |x - origin|^2 * 4^s lies in [2^12, 2^14]: every
+// stored half (coordinates up to 128, -2x up to 256, norm halves up to 2^14)
+// is finite with a 4x margin below FP16's 65504 whatever the data's units, and
+// small-valued data stays clear of the FP16 subnormals.  Scaling by 2^s is
+// exact, so the threshold becomes T * 4^s exactly.  The norms ride in the K
+// padding (d + 4 rounded up to 32), so the MMA yields the (scaled) squared
+// distance directly and the epilogue is one compare per pair.  A pair is
 //   accepted  if D <= T - delta,
 //   rejected  if D >  T + delta,
 //   rechecked otherwise, in FP32 in the reference's order (fma chain),
 // with T the exact squared threshold and delta a per-candidate-row bound on
 // |D - d2_ref| (quantisation error, norm-split residual, tensor-core
 // accumulation error and the reference's own FP32 rounding; derivation in
-// tc_delta_row below).  The result set is therefore identical to the exact path.
+// tc_delta_row below).  A D that is NaN counts as "in the band", never as a
+// reject.  The result set is therefore identical to the exact path.
 //
 // Kernel shape (one CTA per SM, persistent, 96 + 128 * EPI threads):
 //   warp 0      TMA producer: the query block once per work item, candidate
@@ -42,6 +49,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "hj_internal.h"
 #include "hj_tc.cuh"
@@ -136,25 +144,36 @@ __device__ __forceinline__ float tc_delta_row(const TcArgs& a, float4 pc, float 
     return d * 1.01f + 1e-30f;
 }
 
-// Tree minimum of N values with three-input minima.
+// Tree minimum of N values with three-input minima.  The .NaN forms return NaN
+// when any input is NaN, so a NaN accumulator reaches the band test below
+// (where "not above the upper edge" counts it as a hit) instead of being
+// dropped by the minimum.
 __device__ __forceinline__ float fmin3(float a, float b, float c) {
     float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    asm("min.NaN.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
     return r;
 }
+__device__ __forceinline__ float fmin2(float a, float b) {
+    float r;
+    asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+// A value is a candidate hit unless it is known to lie above the band: NaN is
+// kept (and, failing `v <= lo`, goes to the exact recheck).
+__device__ __forceinline__ bool not_above(float v, float hi) { return !(v > hi); }
 template <uint32_t N>
 __device__ __forceinline__ float minN(const float (&v)[N]) {
     if constexpr (N == 1) {
         return v[0];
     } else if constexpr (N == 2) {
-        return fminf(v[0], v[1]);
+        return fmin2(v[0], v[1]);
     } else {
         constexpr uint32_t M = (N + 2) / 3;
         float m[M];
 #pragma unroll
         for (uint32_t i = 0; i < N / 3; ++i) m[i] = fmin3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
         if constexpr (N % 3 == 1) m[M - 1] = v[N - 1];
-        if constexpr (N % 3 == 2) m[M - 1] = fminf(v[N - 2], v[N - 1]);
+        if constexpr (N % 3 == 2) m[M - 1] = fmin2(v[N - 2], v[N - 1]);
         return minN<M>(m);
     }
 }
@@ -464,7 +483,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                             for (uint32_t w = 0; w < W; ++w) load_chunk(v[w], c0 + w);
                             tc::tmem_ld_wait();
     #pragma unroll
-                            for (uint32_t w = 0; w < W; ++w) hitw |= (uint32_t)(minN<LDW>(v[w]) <= hi) << (c0 + w);
+                            for (uint32_t w = 0; w < W; ++w) hitw |= (uint32_t)not_above(minN<LDW>(v[w]), hi) << (c0 + w);
                         }
                         // chunks where some row hit are read again (rare: the accumulator is still
                         // held) and classified pair by pair
@@ -485,7 +504,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     #pragma unroll
                                     for (int i = 0; i < 32; ++i) {
                                         bool inq = cbase + i < ncols;
-                                        hmask |= (uint32_t)(inq && v[h * 32 + i] <= hi) << i;
+                                        hmask |= (uint32_t)(inq && not_above(v[h * 32 + i], hi)) << i;
                                         amask |= (uint32_t)(inq && v[h * 32 + i] <= lo) << i;
                                     }
                                 }
@@ -535,7 +554,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     #pragma unroll
                             for (uint32_t w = 0; w < W; ++w) {
                                 const uint32_t col0 = grp * COLS + (c0 + w) * LDW;
-                                const bool any_hit = minN<LDW>(v[w]) <= hi;
+                                const bool any_hit = not_above(minN<LDW>(v[w]), hi);
                                 if (!__any_sync(0xffffffffu, any_hit)) continue;
     #pragma unroll
                                 for (uint32_t h = 0; h < LDW / 32; ++h) {
@@ -545,7 +564,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     #pragma unroll
                                         for (int i = 0; i < 32; ++i) {
                                             bool inq = cbase + i < ncols;
-                                            hmask |= (uint32_t)(inq && v[w][h * 32 + i] <= hi) << i;
+                                            hmask |= (uint32_t)(inq && not_above(v[w][h * 32 + i], hi)) << i;
                                             amask |= (uint32_t)(inq && v[w][h * 32 + i] <= lo) << i;
                                         }
                                     }
@@ -641,34 +660,80 @@ __device__ __forceinline__ __nv_bfloat16 to_h<__nv_bfloat16>(double x) { return 
 __device__ __forceinline__ double from_h(__half h) { return (double)__half2float(h); }
 __device__ __forceinline__ double from_h(__nv_bfloat16 h) { return (double)__bfloat162float(h); }
 
+// Block-wide maximum of non-negative values, folded into *out with one atomic
+// per block (non-negative IEEE values order like their bit patterns).
+__device__ __forceinline__ void block_max_into(double v, unsigned long long* out) {
+    __shared__ double part[32];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane_id() == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0 && v > 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// Largest |x - origin|^2 over the points, in FP64 (the scale of the operand
+// forms is chosen from it), and whether any coordinate is not finite.
+__global__ void k_tc_range(const float* __restrict__ pts, uint32_t n, uint32_t d, const float* __restrict__ origin,
+                           unsigned long long* __restrict__ max_n2, uint32_t* __restrict__ nonfinite) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double n2 = 0;
+    bool bad = false;
+    if (i < n) {
+        for (uint32_t l = 0; l < d; ++l) {
+            const float v = pts[i * d + l];
+            bad |= !isfinite(v);
+            const double x = (double)v - (double)origin[l];
+            n2 += x * x;
+        }
+    }
+    if (__any_sync(0xffffffffu, bad) && lane_id() == 0) atomicOr(nonfinite, 1u);
+    block_max_into(bad ? 0.0 : n2, max_n2);
+}
+
+// Operand forms of one sorted point (one thread each), in units scaled by
+// `scale` (a power of two): x~ = half((x - origin) * scale).  Also folds the
+// maxima of the per-point bound terms into maxima[0..2] (float bits).
 template <typename H>
 __global__ void k_tc_prep(const float* __restrict__ pts, uint32_t n, uint32_t d, uint32_t kpad,
-                          const float* __restrict__ origin, H* __restrict__ qform, H* __restrict__ cform,
-                          float4* __restrict__ pinfo) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double n2 = 0, e2 = 0;
-    H* qr = qform + (size_t)i * kpad;
-    H* cr = cform + (size_t)i * kpad;
-    for (uint32_t l = 0; l < d; ++l) {
-        double x = (double)pts[(size_t)i * d + l] - (double)origin[l];
-        H h = to_h<H>(x);
-        double xt = from_h(h);
-        e2 += (xt - x) * (xt - x);
-        n2 += xt * xt;
-        qr[l] = h;
-        cr[l] = to_h<H>(-2.0 * xt);
+                          const float* __restrict__ origin, double scale, H* __restrict__ qform,
+                          H* __restrict__ cform, float4* __restrict__ pinfo, unsigned int* __restrict__ maxima) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (i < n) {
+        double n2 = 0, e2 = 0;
+        H* qr = qform + (size_t)i * kpad;
+        H* cr = cform + (size_t)i * kpad;
+        for (uint32_t l = 0; l < d; ++l) {
+            double x = ((double)pts[(size_t)i * d + l] - (double)origin[l]) * scale;   // exact: scale is 2^s
+            H h = to_h<H>(x);
+            double xt = from_h(h);
+            e2 += (xt - x) * (xt - x);
+            n2 += xt * xt;
+            qr[l] = h;
+            cr[l] = to_h<H>(-2.0 * xt);
+        }
+        H nh = to_h<H>(n2);
+        H nl = to_h<H>(n2 - from_h(nh));
+        double res = fabs(n2 - from_h(nh) - from_h(nl));
+        H one = to_h<H>(1.0), zero = to_h<H>(0.0);
+        qr[d] = nh; qr[d + 1] = nl; qr[d + 2] = one; qr[d + 3] = one;
+        cr[d] = one; cr[d + 1] = one; cr[d + 2] = nh; cr[d + 3] = nl;
+        for (uint32_t l = d + 4; l < kpad; ++l) { qr[l] = zero; cr[l] = zero; }
+        // round the bounds up: float conversion is to nearest, so scale by 1 + 2^-20
+        const float up = 1.0f + 9.6e-7f;
+        p = make_float4((float)sqrt(e2) * up, (float)n2 * up, (float)res * up + 1e-30f, 0.f);
+        pinfo[i] = p;
     }
-    H nh = to_h<H>(n2);
-    H nl = to_h<H>(n2 - from_h(nh));
-    double res = fabs(n2 - from_h(nh) - from_h(nl));
-    H one = to_h<H>(1.0), zero = to_h<H>(0.0);
-    qr[d] = nh; qr[d + 1] = nl; qr[d + 2] = one; qr[d + 3] = one;
-    cr[d] = one; cr[d + 1] = one; cr[d + 2] = nh; cr[d + 3] = nl;
-    for (uint32_t l = d + 4; l < kpad; ++l) { qr[l] = zero; cr[l] = zero; }
-    // round the bounds up: float conversion is to nearest, so scale by 1 + 2^-20
-    const float up = 1.0f + 9.6e-7f;
-    pinfo[i] = make_float4((float)sqrt(e2) * up, (float)n2 * up, (float)res * up + 1e-30f, 0.f);
+    float m[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        float v = m[j];
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane_id() == 0 && v > 0.f) atomicMax(&maxima[j], __float_as_uint(v));
+    }
 }
 
 // Per-dimension minimum of the points: lanes walk a row's dimensions (coalesced
@@ -826,7 +891,9 @@ struct TcState {
     int epi = 4;              // epilogue shape code, EPI | 8 * SPLIT (autotuned: 2, 4, 10, 12)
     bool defer = false;       // one vote per accumulator (set from the estimated pair density)
     float gamma_acc = 0;
-    float max_e = 0, max_n = 0, max_r = 0;
+    int scale_exp = 0;        // operand forms hold (x - origin) * 2^scale_exp
+    double thr_s = 0;         // the squared threshold in those units: thr * 4^scale_exp, exact
+    float max_e = 0, max_n = 0, max_r = 0;   // maxima of the per-point bound terms (scaled units)
 };
 
 static TcState* tc_state(const hj_index* ix) { return reinterpret_cast<TcState*>(ix->tc_state); }
@@ -843,65 +910,150 @@ bool tc_supported(const hj_index* ix, int kind) {
 
 uint32_t tc_query_block() { return kQB; }
 
-double tc_delta(const hj_index* ix) {
-    TcState* s = tc_state(ix);
-    if (!s) return 0;
-    double T = ix->thr, sT = std::sqrt(T * (1 + 1e-4));
+// Half-width of the guard band for the worst pair of the dataset, in scaled units.
+static double tc_delta_scaled(const hj_index* ix, const TcState* s) {
+    double T = s->thr_s, sT = std::sqrt(T * (1 + 1e-4));
     double e = 2.0 * s->max_e, ref = (ix->d + 2) * std::ldexp(1.0, -24) * 1.01;
     return (s->gamma_acc * 2.01 * 2 * s->max_n + 2 * s->max_r + e * (2 * sT + 3 * e) + ref * (sT + e) * (sT + e)) * 1.01;
 }
 
+// The same in the dataset's units (the figure the join reports).
+double tc_delta(const hj_index* ix) {
+    TcState* s = tc_state(ix);
+    if (!s) return 0;
+    return std::ldexp(tc_delta_scaled(ix, s), -2 * s->scale_exp);
+}
+
+// Band half-width over the threshold: where it is large the filter decides
+// little and nearly every neighbour goes through the exact recheck.
+double tc_band_ratio(const hj_index* ix) {
+    TcState* s = tc_state(ix);
+    if (!s) return 1e300;
+    return s->thr_s > 0 ? tc_delta_scaled(ix, s) / s->thr_s : 1e300;
+}
+
+int tc_scale_exp(const hj_index* ix) {
+    TcState* s = tc_state(ix);
+    return s ? s->scale_exp : 0;
+}
+
+void tc_release(hj_index* ix) {
+    delete tc_state(ix);
+    ix->tc_state = nullptr;
+}
+
+// Power-of-two exponent s for the operand forms: the largest |x - origin|^2
+// times 4^s lands in (2^12, 2^14], and the threshold times 4^s stays a normal
+// float (so scaling it is exact).  Returns false when both cannot hold.
+static bool choose_scale(double max_n2, double thr, int* out) {
+    int s = 0;
+    if (max_n2 > 0) {
+        int e2 = 0;
+        std::frexp(max_n2, &e2);                 // max_n2 in [2^(e2-1), 2^e2)
+        s = (14 - e2) >> 1;                      // floor((14 - e2) / 2)
+        while (s > -600 && std::ldexp(max_n2, 2 * s) > 16384.0) --s;
+        while (s < 600 && std::ldexp(max_n2, 2 * s + 2) <= 16384.0) ++s;
+    }
+    if (thr > 0) {
+        // keep T * 4^s within [2^-100, 2^100]: exact in float and far from overflow
+        while (std::ldexp(thr, 2 * s) > std::ldexp(1.0, 100)) --s;
+        if (std::ldexp(thr, 2 * s) < std::ldexp(1.0, -100)) return false;
+    }
+    if (max_n2 > 0 && std::ldexp(max_n2, 2 * s) > 16384.0 * 1.0001) return false;
+    *out = s;
+    return true;
+}
+
 hj_status tc_prepare(hj_index* ix, int kind, cudaStream_t st) {
     if (ix->tc_kind == kind && ix->tc_state) return HJ_OK;
-    const uint32_t kpad = kpad_for(ix->d), n = ix->n, d = ix->d;
+    // Drop the previous operand forms before anything else: if a step below
+    // fails, no tensor map may be left pointing at freed buffers.
+    tc_release(ix);
+    ix->tc_kind = -1;
     dfree(ix->tc_a, st);
     dfree(ix->tc_b, st);
     dfree(ix->tc_err, st);
+    const uint32_t kpad = kpad_for(ix->d), n = ix->n, d = ix->d;
     uint16_t *qf = nullptr, *cf = nullptr;
     float* origin = nullptr;
     float4* pinfo = nullptr;
-    HJ_TRY(dalloc(&qf, (size_t)n * kpad, st));
-    HJ_TRY(dalloc(&cf, (size_t)n * kpad, st));
-    HJ_TRY(dalloc(&pinfo, n, st));
-    HJ_TRY(dalloc(&origin, d, st));
+    unsigned long long* rng = nullptr;   // [0] max |x - origin|^2 (FP64 bits), [1] non-finite flag
+    unsigned int* mx = nullptr;          // maxima of the bound terms (float bits)
+    auto fail = [&](hj_status e) {
+        cudaGetLastError();
+        dfree(qf, st); dfree(cf, st); dfree(pinfo, st); dfree(origin, st); dfree(rng, st); dfree(mx, st);
+        return e;
+    };
+#define TC_TRY(x) do { hj_status e_ = (x); if (e_ != HJ_OK) return fail(e_); } while (0)
+    TC_TRY(dalloc(&qf, (size_t)n * kpad, st));
+    TC_TRY(dalloc(&cf, (size_t)n * kpad, st));
+    TC_TRY(dalloc(&pinfo, n, st));
+    TC_TRY(dalloc(&origin, d, st));
+    TC_TRY(dalloc(&rng, 2, st));
+    TC_TRY(dalloc(&mx, 4, st));
+    TC_TRY(cuda_status(cudaMemsetAsync(rng, 0, 2 * sizeof(unsigned long long), st), "clear range scratch"));
+    TC_TRY(cuda_status(cudaMemsetAsync(mx, 0, 4 * sizeof(unsigned int), st), "clear maxima"));
     k_fill_f32<<<(d + 255) / 256, 256, 0, st>>>(origin, d, INFINITY);
-    HJ_LAUNCHED();
+    TC_TRY(launch_status(__FILE__, __LINE__));
     {
         const unsigned blocks = (unsigned)std::min<uint32_t>(num_sms() * 2, std::max<uint32_t>(1, n / 64));
         k_col_min<<<blocks, 256, (size_t)8 * d * sizeof(float), st>>>((const float*)ix->pts, n, d, origin);
-        HJ_LAUNCHED();
+        TC_TRY(launch_status(__FILE__, __LINE__));
     }
+    const unsigned pblocks = std::max<uint32_t>(1, (n + 255) / 256);
+    k_tc_range<<<pblocks, 256, 0, st>>>((const float*)ix->pts, n, d, origin, rng,
+                                        reinterpret_cast<uint32_t*>(rng + 1));
+    TC_TRY(launch_status(__FILE__, __LINE__));
+    unsigned long long hr[2] = {0, 0};
+    TC_TRY(cuda_status(cudaMemcpyAsync(hr, rng, sizeof(hr), cudaMemcpyDeviceToHost, st), "range to host"));
+    TC_TRY(cuda_status(cudaStreamSynchronize(st), "range sync"));
+    if (hr[1]) {
+        set_error("the tensor-core filter needs finite coordinates (the dataset holds inf or NaN)");
+        return fail(HJ_ERR_UNSUPPORTED);
+    }
+    double max_n2 = 0;
+    std::memcpy(&max_n2, &hr[0], sizeof(double));
+    int sexp = 0;
+    if (!choose_scale(max_n2, ix->thr, &sexp)) {
+        set_error("the tensor-core filter cannot scale this dataset: eps^2 / max |x - min|^2 = %g is below 2^-114",
+                  ix->thr / max_n2);
+        return fail(HJ_ERR_UNSUPPORTED);
+    }
+    const double scale = std::ldexp(1.0, sexp);
     if (kind == HJ_REFINE_TC_BF16)
-        k_tc_prep<__nv_bfloat16><<<(n + 255) / 256, 256, 0, st>>>((const float*)ix->pts, n, d, kpad, origin,
-                                                                   (__nv_bfloat16*)qf, (__nv_bfloat16*)cf, pinfo);
+        k_tc_prep<__nv_bfloat16><<<pblocks, 256, 0, st>>>((const float*)ix->pts, n, d, kpad, origin, scale,
+                                                           (__nv_bfloat16*)qf, (__nv_bfloat16*)cf, pinfo, mx);
     else
-        k_tc_prep<__half><<<(n + 255) / 256, 256, 0, st>>>((const float*)ix->pts, n, d, kpad, origin, (__half*)qf,
-                                                            (__half*)cf, pinfo);
-    HJ_LAUNCHED();
+        k_tc_prep<__half><<<pblocks, 256, 0, st>>>((const float*)ix->pts, n, d, kpad, origin, scale, (__half*)qf,
+                                                    (__half*)cf, pinfo, mx);
+    TC_TRY(launch_status(__FILE__, __LINE__));
+    unsigned int hm[4] = {0, 0, 0, 0};
+    TC_TRY(cuda_status(cudaMemcpyAsync(hm, mx, sizeof(hm), cudaMemcpyDeviceToHost, st), "maxima to host"));
+    TC_TRY(cuda_status(cudaStreamSynchronize(st), "maxima sync"));
+    TcMaps maps;
+    TC_TRY(make_map(&maps.query, qf, n, kpad, kind));
+    TC_TRY(make_map(&maps.cand, cf, n, kpad, kind));
+#undef TC_TRY
     dfree(origin, st);
-    ix->tc_a = qf;
-    ix->tc_b = cf;
-    ix->tc_err = reinterpret_cast<float*>(pinfo);
-    ix->tc_kpad = kpad;
-    ix->tc_kind = kind;
-    if (!ix->tc_state) ix->tc_state = new TcState();
-    TcState* s = tc_state(ix);
-    HJ_TRY(make_map(&s->maps.query, qf, n, kpad, kind));
-    HJ_TRY(make_map(&s->maps.cand, cf, n, kpad, kind));
+    dfree(rng, st);
+    dfree(mx, st);
+    TcState* s = new TcState();
+    s->maps = maps;
     // Accumulation model: each K=16 MMA step adds 16 exact products to the FP32
     // accumulator with at most 2 ulps of the largest magnitude per term lost
     // (alignment and truncation); bound = (steps + 1) * 32 * 2^-23 * sum|terms|.
     s->gamma_acc = (float)((kpad / 16 + 1) * 32 * std::ldexp(1.0, -23));
-    // global maxima of the per-point terms, for the reported delta
-    std::vector<float4> hp(n);
-    HJ_CUDA(cudaMemcpyAsync(hp.data(), pinfo, (size_t)n * sizeof(float4), cudaMemcpyDeviceToHost, st));
-    HJ_CUDA(cudaStreamSynchronize(st));
-    s->max_e = s->max_n = s->max_r = 0;
-    for (const float4& p : hp) {
-        s->max_e = std::max(s->max_e, p.x);
-        s->max_n = std::max(s->max_n, p.y);
-        s->max_r = std::max(s->max_r, p.z);
-    }
+    s->scale_exp = sexp;
+    s->thr_s = std::ldexp(ix->thr, 2 * sexp);
+    std::memcpy(&s->max_e, &hm[0], 4);
+    std::memcpy(&s->max_n, &hm[1], 4);
+    std::memcpy(&s->max_r, &hm[2], 4);
+    ix->tc_a = qf;
+    ix->tc_b = cf;
+    ix->tc_err = reinterpret_cast<float*>(pinfo);
+    ix->tc_kpad = kpad;
+    ix->tc_state = s;
+    ix->tc_kind = kind;
     return HJ_OK;
 }
 
@@ -917,11 +1069,6 @@ void tc_set_epi(hj_index* ix, int epi) {
 void tc_set_defer(hj_index* ix, bool defer) {
     TcState* s = tc_state(ix);
     if (s) s->defer = defer;
-}
-
-void tc_release(hj_index* ix) {
-    delete tc_state(ix);
-    ix->tc_state = nullptr;
 }
 
 hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t nblocks, unsigned int* head,
@@ -952,9 +1099,9 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     a.hash = cell_hash(ix);
     a.pinfo = reinterpret_cast<const float4*>(ix->tc_err);
     a.n = ix->n; a.nkb = nkb; a.stages = stages;
-    a.thr = (float)ix->thr;
+    a.thr = (float)s->thr_s;   // exact: thr * 4^s
     a.gamma_acc = s->gamma_acc;
-    a.s_t = (float)(std::sqrt(ix->thr * (1 + 1e-4)) * (1 + 1e-6));
+    a.s_t = (float)(std::sqrt(s->thr_s * (1 + 1e-4)) * (1 + 1e-6));
     a.ref_rel = (float)((ix->d + 2) * std::ldexp(1.0, -24) * 1.01);
     a.sink = sink; a.band = band;
     a.count_only = count_only; a.block_counts = block_counts; a.stats = stats; a.err = err;
@@ -1007,5 +1154,13 @@ extern "C" hj_status hj_probe_tc_tile(hj_index* ix, int kind, uint32_t a0, uint3
     HJ_CUDA(cudaStreamSynchronize(st));
     dfree(err, st);
     if (herr) { set_error("hj_probe_tc_tile: a bounded wait expired"); return HJ_ERR_TIMEOUT; }
+    return HJ_OK;
+}
+
+extern "C" hj_status hj_tc_operand_scale(const hj_index* ix, int* log2_scale) {
+    using namespace hj;
+    if (!ix || !log2_scale) { set_error("hj_tc_operand_scale: null argument"); return HJ_ERR_INVALID; }
+    if (!ix->tc_state) { set_error("hj_tc_operand_scale: no tensor-core operands prepared"); return HJ_ERR_INVALID; }
+    *log2_scale = tc_scale_exp(ix);
     return HJ_OK;
 }

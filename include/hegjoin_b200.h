@@ -135,14 +135,15 @@ hj_status hj_grid_geometry(const void* d_db, uint32_t n, uint32_t d, uint32_t k,
 /* The same geometry without any device allocation; it has no counterpart in
  * the reference.  For callers that cannot allocate device memory where they
  * need the geometry: a process that reserves all of its device memory up
- * front and must not fail on an allocation later, or code running while a
- * stream is being captured (cudaMalloc is not allowed then).  Its scratch is a
- * file-scope device array of 151,808 bytes (k <= 16 indexed dimensions, any
- * n) that every GPU loading the library keeps until exit; larger k is rejected
- * with HJ_ERR_INVALID.  All calls on a device share that array, so calls that
- * overlap on the GPU race: serialise them.  The first call on a device looks
- * up the array's address; make it before any stream capture.  Synchronises
- * `stream`. */
+ * front (a server sized to a fixed HBM budget, or a job under a fixed quota)
+ * and must not fail on an allocation later.  Its scratch is a file-scope
+ * device array of 151,808 bytes (k <= 16 indexed dimensions, any n) that every
+ * GPU loading the library keeps until exit; larger k is rejected with
+ * HJ_ERR_INVALID.  All calls on a device share that array, so calls that
+ * overlap on the GPU race: serialise them.  The first call on a device (and
+ * the first after that device's context changes) looks up the array's
+ * address.  The call copies its result to the host and synchronises `stream`,
+ * so it must not be made on a stream that is being captured. */
 hj_status hj_grid_geometry_noalloc(const void* d_db, uint32_t n, uint32_t d, uint32_t k, int dtype,
                                    double eps, double* h_min_arr, double* h_max_arr,
                                    uint32_t* h_n_cells, uint64_t* h_total_cells, void* stream);
@@ -270,9 +271,17 @@ hj_status hj_probe_sqdist(const void* d_a, const void* d_b, uint32_t n, uint32_t
  * and tcgen05 path, writing the 128 x 512 FP32 accumulators (row = candidate,
  * column = query) to d_out.  Optionally copies the quantised operand rows
  * (query form 512 x kpad and candidate form 128 x kpad, 16-bit, kpad =
- * 32 * ceil((d + 4) / 32)) to host buffers.  Synchronises `stream`. */
+ * 32 * ceil((d + 4) / 32)) to host buffers.  Synchronises `stream`.  The
+ * operand rows and accumulators are in the filter's scaled units: divide rows
+ * by 2^s and accumulators by 4^s, s from hj_tc_operand_scale. */
 hj_status hj_probe_tc_tile(hj_index* ix, int refine_kind, uint32_t a0, uint32_t b0, float* d_out,
                            void* h_query_rows, void* h_cand_rows, void* stream);
+
+/* The power-of-two exponent s of the tensor-core operand forms last prepared
+ * for this index: they hold (x - min) * 2^s, chosen per dataset so that every
+ * stored half is finite.  Internal to the filter (no reference counterpart);
+ * exposed for the probes and tests. */
+hj_status hj_tc_operand_scale(const hj_index* ix, int* log2_scale);
 
 #ifdef __cplusplus
 }

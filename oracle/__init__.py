@@ -38,6 +38,8 @@ def _load():
         getattr(lib, f"hjo_join_{suf}").restype = U64
         getattr(lib, f"hjo_join_sample_{suf}").argtypes = [P, U32, U32, U32, T, P, P, P, U32, P]
         getattr(lib, f"hjo_join_sample_{suf}").restype = U64
+        getattr(lib, f"hjo_join_lists_{suf}").argtypes = [P, U32, U32, U32, T, P, P, P, U32, P, P, U64]
+        getattr(lib, f"hjo_join_lists_{suf}").restype = U64
         getattr(lib, f"hjo_sqdist_{suf}").argtypes = [P, P, U32, I]
         getattr(lib, f"hjo_sqdist_{suf}").restype = D
     lib.hjo_ref_cell_order.argtypes = [P, U32, P]
@@ -136,6 +138,26 @@ def join_sample(db: np.ndarray, k: int, eps, qids: np.ndarray, min_arr=None, n_c
     pairs = getattr(lib, f"hjo_join_sample_{_suf(db)}")(_p(db), n, d, k, db.dtype.type(eps), _p(mn), _p(nc), _p(q),
                                                        len(q), ctypes.byref(sec))
     return int(pairs), float(sec.value)
+
+
+def join_lists(db: np.ndarray, k: int, eps, qids: np.ndarray, min_arr=None, n_cells=None):
+    """Neighbour lists of the sampled query ids: (counts[len(qids)], concatenated sorted lists)."""
+    db = np.ascontiguousarray(db)
+    n, d = db.shape
+    if min_arr is None or n_cells is None:
+        min_arr, _, n_cells, _ = geometry(db, k, eps)
+    mn = np.ascontiguousarray(min_arr, dtype=db.dtype)
+    nc = np.ascontiguousarray(n_cells, dtype=np.uint32)
+    q = np.ascontiguousarray(qids, dtype=np.uint32)
+    counts = np.zeros(len(q), np.uint32)
+    fn = getattr(lib, f"hjo_join_lists_{_suf(db)}")
+    cap = max(1, 256 * len(q))
+    while True:
+        vals = np.zeros(cap, np.uint32)
+        total = fn(_p(db), n, d, k, db.dtype.type(eps), _p(mn), _p(nc), _p(q), len(q), _p(counts), _p(vals), cap)
+        if total <= cap:
+            return counts, vals[:total]
+        cap = int(total)
 
 
 def digest(off: np.ndarray, vals: np.ndarray):

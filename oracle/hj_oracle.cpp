@@ -280,6 +280,48 @@ HJO_JOIN(double, f64)
 HJO_JOIN_SAMPLE(float, f32)
 HJO_JOIN_SAMPLE(double, f64)
 
+// The join's neighbour lists for a sample of query ids (kernel.cu:727-802, as
+// hjo_join): counts[s] for query qids[s], and, when the lists fit `capacity`,
+// the lists themselves (each sorted ascending) concatenated in sample order.
+// Returns the total list length; the caller re-calls with a larger buffer when
+// it exceeds `capacity` (vals is then left untouched).
+#define HJO_JOIN_LISTS(T, SUF)                                                                       \
+    uint64_t hjo_join_lists_##SUF(const T* db, uint32_t n, uint32_t d, uint32_t k, T eps,             \
+                                  const T* minArr, const uint32_t* nCells, const uint32_t* qids,     \
+                                  uint32_t nq, uint32_t* counts, uint32_t* vals, uint64_t capacity) { \
+        Index ix;                                                                                    \
+        build_index<T>(db, n, d, k, eps, minArr, nCells, ix);                                        \
+        std::vector<std::vector<uint32_t>> lists(nq);                                                \
+        _Pragma("omp parallel for schedule(dynamic, 1)")                                             \
+        for (int64_t s = 0; s < (int64_t)nq; ++s) {                                                  \
+            const T* p = db + (size_t)qids[s] * d;                                                   \
+            std::vector<uint32_t>& L = lists[s];                                                     \
+            for_each_stencil_cell<T>(p, k, eps, minArr, nCells, ix, [&](int64_t ci) {                \
+                for (int32_t j = ix.first[ci]; j <= ix.last[ci]; ++j) {                              \
+                    uint32_t cid = ix.lookup[j];                                                     \
+                    T acc = sqdist<T>(db + (size_t)cid * d, p, d, 1);                                \
+                    if (std::sqrt(acc) <= eps) L.push_back(cid);                                     \
+                }                                                                                    \
+            });                                                                                      \
+            std::sort(L.begin(), L.end());                                                           \
+        }                                                                                            \
+        uint64_t total = 0;                                                                          \
+        for (uint32_t s = 0; s < nq; ++s) {                                                          \
+            counts[s] = (uint32_t)lists[s].size();                                                   \
+            total += lists[s].size();                                                                \
+        }                                                                                            \
+        if (vals && total <= capacity) {                                                             \
+            uint64_t w = 0;                                                                          \
+            for (uint32_t s = 0; s < nq; ++s) {                                                      \
+                std::memcpy(vals + w, lists[s].data(), lists[s].size() * 4);                         \
+                w += lists[s].size();                                                                \
+            }                                                                                        \
+        }                                                                                            \
+        return total;                                                                                \
+    }
+HJO_JOIN_LISTS(float, f32)
+HJO_JOIN_LISTS(double, f64)
+
 // Squared distance of one pair in the reference order (for error statistics).
 double hjo_sqdist_f32(const float* a, const float* b, uint32_t d, int fma_mode) {
     return (double)sqdist<float>(a, b, d, fma_mode);

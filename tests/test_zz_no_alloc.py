@@ -2,8 +2,8 @@
 
 It exists for callers that cannot allocate device memory at the point where
 they need the grid geometry -- a process that reserves all of its device memory
-up front, or code running while a stream is being captured -- so its scratch is
-a static device array shared by every call.  Called through the C ABI twice in
+up front and must not fail on an allocation later -- so its scratch is a static
+device array shared by every call.  Called through the C ABI twice in
 a row, on different data, it must return exactly what the allocating entry
 point (hj_grid_geometry) returns: dataset-type minima and integer cell counts,
 so the tolerance is zero.  k beyond the array's limit must be rejected.  This
