@@ -163,15 +163,36 @@ def cpu_baseline(db, wl, seconds_target=20.0):
                       f"refine only, the index is built untimed"}
 
 
+def load_workloads():
+    """hegjoin_b200/workloads.py loaded by path: the workload table and the host
+    generator (libhj_datagen.so) without importing the package, so the
+    reference arm never loads the GPU library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("hj_workloads", os.path.join(ROOT, "hegjoin_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod      # dataclasses look their module up while the class is built
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config(wl):
+    """The `config` both arms print for a workload (identical keys and values)."""
+    return {"workload": wl.name, "n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps, "dtype": wl.dtype,
+            "seed": wl.seed, "l2": f"inputs larger than L2 ({wl.n * wl.d * (4 if wl.dtype == 'f32' else 8) / 1e6:.0f} "
+                                  f"MB dataset > 126 MB L2); no flush"}
+
+
 def reference_arm(args, wl):
-    ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     db = wl.generate()
+    # each step a bounded sample, so the whole run stays within a few minutes
+    per_step = max(3.0, min(args.ref_seconds, 150.0 / max(1, args.steps + args.warmup)))
     steps = []
     base = None
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline(db, wl, seconds_target=args.ref_seconds)
+        b = cpu_baseline(db, wl, seconds_target=per_step)
         if i >= args.warmup:
             steps.append(b)
         base = b
@@ -179,8 +200,8 @@ def reference_arm(args, wl):
     line = {"impl": "reference", "metric": "result pairs/s", "value": val, "unit": "pairs/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic (seeded Exp(40) generator)",
-            "config": {"workload": wl.name, "n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps,
-                       "sample_per_step": base["sample"]},
+            "config": workload_config(wl),
+            "run": {"sample_per_step": base["sample"], "seconds_per_step_target": per_step},
             "cpu_baseline": {**base, "value": val},
             "e2e": {"value": val, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -205,25 +226,33 @@ def quick_eps(db: np.ndarray, target: float, dev, seed: int) -> float:
     return float(np.float32(np.sqrt(max(r2, 1e-12))))
 
 
-def serve_bench(args):
+def serving_run(n_requests: int, max_n: int, min_n: int = 1000, workers: int = 8, load: float = 5.0,
+                hbm_budget_gb: float = 150.0, seed: int = 5, refine: str = "auto", with_plain: bool = True):
+    """A seeded request stream through the serving loop: n log-uniform in [min_n, max_n],
+    d from {2, 6, 18, 32, 90} (k = min(d, 6)), eps per request for a mean neighbour count
+    drawn from U[4, 128].  Measures, on the same requests:
+      serial        the same engine, one request at a time (all queued at t = 0, 1 worker);
+      serial_plain  plain FP32 joins (exact refine), one at a time;
+      capacity      all requests queued at once, `workers` in flight;
+      served        Poisson arrivals at `load` x the serial same-engine request rate.
+    Latency is per request, from submit to completion."""
     import threading
     import torch
     import hegjoin_b200 as hj
     dev = torch.device("cuda", 0)
-    rng = np.random.default_rng(args.serve_seed)
+    rng = np.random.default_rng(seed)
     reqs = []
-    for i in range(args.requests):
-        n = int(np.exp(rng.uniform(np.log(1e3), np.log(args.max_n))))
+    for i in range(n_requests):
+        n = int(np.exp(rng.uniform(np.log(min_n), np.log(max_n))))
         d = int(rng.choice([2, 6, 18, 32, 90]))
         target = float(rng.uniform(4, 128))
         db = hj.generate_exp40(10_000 + i, n, d, np.float32)
         reqs.append((db, min(d, 6), quick_eps(db, target, dev, i), target))
     total_pts = sum(r[0].shape[0] for r in reqs)
 
-    def run(workers, arrivals, todo=None, refine=None):
+    def run(nworkers, arrivals, todo=None, refine_kind=None):
         todo = reqs[:len(arrivals)] if todo is None else todo
-        srv = hj.Server(workers=workers, hbm_budget=int(args.hbm_budget_gb * (1 << 30)),
-                        refine=refine or args.refine)
+        srv = hj.Server(workers=nworkers, hbm_budget=int(hbm_budget_gb * (1 << 30)), refine=refine_kind or refine)
         tickets = [None] * len(todo)
         t0 = time.perf_counter()
 
@@ -239,7 +268,7 @@ def serve_bench(args):
         lat, pairs, infos = [], 0, []
         for i in range(len(todo)):
             while tickets[i] is None:
-                time.sleep(0.0005)
+                time.sleep(0.0002)
             _, info = srv.wait(tickets[i], keep_result=False)
             lat.append(info.t_done - info.t_submit)
             pairs += info.stats.total_pairs
@@ -248,6 +277,7 @@ def serve_bench(args):
         span = max(x.t_done for x in infos) - min(x.t_submit for x in infos)
         srv.close()
         return {"pairs": int(pairs), "seconds": span, "pairs_per_s": pairs / span,
+                "requests_per_s": len(todo) / span,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "mean_ms": float(np.mean(lat) * 1e3)}
 
@@ -256,101 +286,125 @@ def serve_bench(args):
     for r in reqs:
         first.setdefault(r[0].shape[1], r)
     run(1, np.zeros(len(first)), list(first.values()))
-    run(1, np.zeros(len(first)), list(first.values()), refine="exact")
-    # one request at a time, all queued at t=0: plain FP32 joins, and the same engine's choice
-    serial_plain = run(1, np.zeros(len(reqs)), refine="exact")
+    run(1, np.zeros(len(first)), list(first.values()), refine_kind="exact")
     serial = run(1, np.zeros(len(reqs)))
-    capacity = run(args.workers, np.zeros(len(reqs)))      # everything queued at once
-    # Poisson arrivals at `load` times the serial plain request rate
-    rate = args.load * len(reqs) / serial_plain["seconds"]
+    serial_plain = run(1, np.zeros(len(reqs)), refine_kind="exact") if with_plain else None
+    capacity = run(workers, np.zeros(len(reqs)))
+    rate = load * len(reqs) / serial["seconds"]
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
-    served = run(args.workers, arrivals)
+    served = run(workers, arrivals)
     served["offered_seconds"] = float(arrivals[-1])
-    line = {"metric": "served p50/p99 latency (ms) and aggregate result pairs/s", "value": served["pairs_per_s"],
+    out = {"requests": len(reqs), "points_total": int(total_pts), "n_range": [min_n, max_n],
+           "d_choices": [2, 6, 18, 32, 90], "k": "min(d, 6)", "target_neighbours": "U[4, 128]",
+           "arrivals": "Poisson", "offered_rate_req_per_s": rate,
+           "offered_load": f"{load} x the serial same-engine request rate", "workers": workers,
+           "hbm_budget_gb": hbm_budget_gb, "refine": refine,
+           "served": served, "capacity": capacity, "serial": serial,
+           "capacity_vs_serial": capacity["pairs_per_s"] / serial["pairs_per_s"],
+           "served_vs_serial": served["pairs_per_s"] / serial["pairs_per_s"],
+           "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"]}
+    if serial_plain:
+        out["serial_plain"] = serial_plain
+        out["capacity_vs_serial_plain"] = capacity["pairs_per_s"] / serial_plain["pairs_per_s"]
+        out["served_vs_serial_plain"] = served["pairs_per_s"] / serial_plain["pairs_per_s"]
+    return out
+
+
+def serve_bench(args):
+    with ClockSampler(0) as clk:
+        r = serving_run(args.requests, args.max_n, args.min_n, args.workers, args.load, args.hbm_budget_gb,
+                        args.serve_seed, args.refine)
+    line = {"metric": "served p50/p99 latency (ms) and aggregate result pairs/s", "value": r["served"]["pairs_per_s"],
             "unit": "pairs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
-            "data": "synthetic request stream (seeded Exp(40) datasets)",
-            "config": {"workload": "serving", "requests": len(reqs), "points_total": int(total_pts),
-                       "n_range": [1000, args.max_n], "d_choices": [2, 6, 18, 32, 90], "k": "min(d, 6)",
-                       "target_neighbours": "U[4, 128]", "arrivals": "Poisson",
-                       "offered_rate_req_per_s": rate,
-                       "offered_load": f"{args.load} x the serial plain request rate",
-                       "workers": args.workers, "hbm_budget_gb": args.hbm_budget_gb, "refine": args.refine},
-            "served": served, "capacity": capacity, "serial": serial, "serial_plain": serial_plain,
-            "speedup_vs_serial_plain": served["pairs_per_s"] / serial_plain["pairs_per_s"],
-            "speedup_vs_serial": served["pairs_per_s"] / serial["pairs_per_s"],
-            "capacity_vs_serial": capacity["pairs_per_s"] / serial["pairs_per_s"],
-            "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"]}
+            "data": "synthetic request stream (seeded Exp(40) datasets)", "config": {"workload": "serving"},
+            **r, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------------------------------------
 # tensor-core filter vs plain FP32 refine on one workload: --compare
-def compare_bench(args, wl):
+def tc_vs_plain(wl, steps: int, warmup: int, tc_kind: str = "auto"):
+    """The exact refine (plain FP32 on the CUDA cores) against the tensor-core
+    filter on one workload: whole steps (index, workload order, join) timed with
+    CUDA events on the launching stream, pair sets compared through per-query
+    digests, and the filter's squared-distance error against FP64 on sampled tiles."""
     import torch
     import hegjoin_b200 as hj
     dev = torch.device("cuda", 0)
     np_db = wl.generate()
     db = torch.from_numpy(np_db).to(dev)
-    out = {}
-    digests = {}
-    for refine in ("exact", args.tc_kind):
-        times, launches0 = [], hj.kernel_launch_count()
-        for it in range(args.warmup + args.steps):
+    stream = torch.cuda.current_stream(dev)
+    out, digests = {}, {}
+    for refine in ("exact", tc_kind):
+        ms = []
+        for it in range(warmup + steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
+            e0.record(stream)
             ix = hj.GridIndex(db, wl.k, wl.eps)
             cand = ix.sort_by_workload()
             res = hj.join(ix, refine=refine)
+            e1.record(stream)
             torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            if it >= args.warmup:
-                times.append(t1 - t0)
+            if it >= warmup:
+                ms.append(e0.elapsed_time(e1))
             st = res.stats
-            if it == args.warmup + args.steps - 1:
-                c, s, x = res.digest()
-                digests[refine] = (c.cpu().numpy(), s.cpu().numpy(), x.cpu().numpy())
+            if it == warmup + steps - 1:
+                c, s_, x = res.digest()
+                digests[refine] = (c.cpu().numpy(), s_.cpu().numpy(), x.cpu().numpy())
             res.close()
             ix.close()
-        sec = statistics.mean(times)
+        sec = statistics.mean(ms) / 1e3
         out[refine] = {"pairs": int(st.total_pairs), "seconds_per_step": sec, "pairs_per_s": st.total_pairs / sec,
+                       "refine_used": {1: "exact", 2: "tc_f16", 3: "tc_bf16"}.get(int(st.refine_used)),
                        "refine_kernel_ms": st.ms_refine_kernel,
                        "join_ms": {"estimate": st.ms_estimate, "refine": st.ms_refine, "group": st.ms_group,
                                    "total": st.ms_total},
                        "batches": int(st.n_batches), "retries": int(st.n_retries), "band_pairs": int(st.band_pairs),
                        "tc_accepts": int(st.tc_accepts), "filter_delta": st.filter_delta,
                        "candidates": int(cand)}
-    same = all(np.array_equal(a, b) for a, b in zip(digests["exact"], digests[args.tc_kind]))
+    same = all(np.array_equal(a, b) for a, b in zip(digests["exact"], digests[tc_kind]))
     # max |D - d2_fp64| of the tensor-core squared distance over sampled tiles
+    probe_kind = out[tc_kind]["refine_used"] if out[tc_kind]["refine_used"] != "exact" else "tc_f16"
     ix = hj.GridIndex(db, wl.k, wl.eps)
     ix.sort_by_workload()
     n = np_db.shape[0]
     torch.cuda.synchronize()
     P = hj.device_view(ix.views()[0], (n, wl.d), np.float32).double().cpu().numpy()   # points in cell order
     rng = np.random.default_rng(3)
-    max_err, max_rel = 0.0, 0.0
+    max_err, max_near = 0.0, 0.0
     for _ in range(16):
         a0 = int(rng.integers(0, max(1, n - 128)))
         b0 = int(rng.integers(0, max(1, n - 512)))
-        acc, _, _ = hj.probe_tc_tile(ix, args.tc_kind, a0, b0)
+        acc, _, _ = hj.probe_tc_tile(ix, probe_kind, a0, b0)
         nc, nq = min(128, n - a0), min(512, n - b0)
         C = P[a0:a0 + nc]
         Q = P[b0:b0 + nq]
         d2 = ((C[:, None, :] - Q[None, :, :]) ** 2).sum(-1)
-        err = np.abs(acc[:nc, :nq].astype(np.float64) - d2)
+        err = np.abs(acc[:nc, :nq] - d2)
         near = d2 <= 4 * wl.eps * wl.eps
         max_err = max(max_err, float(err.max()))
         if near.any():
-            max_rel = max(max_rel, float(err[near].max()))
+            max_near = max(max_near, float(err[near].max()))
     ix.close()
-    line = {"metric": "result pairs/s, tensor-core filter vs plain FP32", "workload": wl.name,
-            "config": {"n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps, "steps": args.steps, "warmup": args.warmup},
-            "exact": out["exact"], "tc": out[args.tc_kind], "tc_kind": args.tc_kind,
-            "speedup": out[args.tc_kind]["pairs_per_s"] / out["exact"]["pairs_per_s"],
+    del db
+    torch.cuda.empty_cache()
+    return {"workload": wl.name, "n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps, "steps": steps, "warmup": warmup,
+            "timing": "whole steps (index + workload order + join), CUDA events on the launching stream",
+            "plain_fp32": out["exact"], "tc_filter": out[tc_kind],
+            "speedup": out[tc_kind]["pairs_per_s"] / out["exact"]["pairs_per_s"],
             "identical_pair_sets": bool(same),
-            "max_abs_d2_error_vs_fp64": max_err, "max_abs_d2_error_vs_fp64_within_2eps": max_rel,
-            "filter_delta": out[args.tc_kind]["filter_delta"],
-            "error_sample": "16 random tiles of 128 candidates x 512 queries (tile probe) vs FP64 distances"}
-    print(json.dumps(line), flush=True)
+            "band_pairs": out[tc_kind]["band_pairs"], "filter_delta": out[tc_kind]["filter_delta"],
+            "max_abs_d2_error_vs_fp64": max_err, "max_abs_d2_error_vs_fp64_within_2eps": max_near,
+            "error_sample": f"16 random tiles of 128 candidates x 512 queries ({probe_kind} tile probe) "
+                            f"against FP64 distances"}
+
+
+def compare_bench(args, wl):
+    with ClockSampler(0) as clk:
+        r = tc_vs_plain(wl, args.steps, args.warmup, args.tc_kind)
+    print(json.dumps({"metric": "result pairs/s, tensor-core filter vs plain FP32", **r, "clocks": clk.summary()}),
+          flush=True)
 
 
 def main():
@@ -364,24 +418,28 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="override the workload's point count (testing only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the tensor-core-vs-plain (90-D) and serving blocks of the default line")
+    ap.add_argument("--extra-steps", type=int, default=2)
     ap.add_argument("--ref-seconds", type=float, default=20.0)
     ap.add_argument("--serve", action="store_true", help="run the request-stream serving benchmark instead")
     ap.add_argument("--requests", type=int, default=256)
+    ap.add_argument("--min-n", type=int, default=1000)
     ap.add_argument("--max-n", type=int, default=1_000_000)
     ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--load", type=float, default=5.0,
-                    help="serving: Poisson arrival rate as a multiple of the serial plain-join request rate")
+                    help="serving: Poisson arrival rate as a multiple of the serial same-engine request rate")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-seed", type=int, default=5)
     ap.add_argument("--compare", action="store_true", help="time the exact refine against the tensor-core filter")
-    ap.add_argument("--tc-kind", default="tc_f16", choices=["tc_f16", "tc_bf16"])
+    ap.add_argument("--tc-kind", default="auto", choices=["auto", "tc_f16", "tc_bf16"])
     args = ap.parse_args()
     if args.serve:
         serve_bench(args)
         return
 
-    from hegjoin_b200 import workloads
-    wl = workloads.WORKLOADS[args.workload]
+    wlmod = load_workloads()
+    wl = wlmod.WORKLOADS[args.workload]
     if args.n:
         import dataclasses
         wl = dataclasses.replace(wl, n=args.n)
@@ -518,21 +576,34 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(np_db, wl, seconds_target=20.0)
 
+    # the north-star comparisons, each with its own clock record (single GPU only)
+    extras = {}
+    if ws == 1 and not args.no_extras:
+        del db
+        torch.cuda.empty_cache()
+        with ClockSampler(local) as clk3:
+            extras["tc_vs_plain"] = tc_vs_plain(wlmod.WORKLOADS["c3_90d"], args.extra_steps, 1)
+        extras["tc_vs_plain"]["clocks"] = clk3.summary()
+        with ClockSampler(local) as clk5:
+            extras["serving"] = serving_run(96, 100_000, workers=8, load=5.0, seed=args.serve_seed)
+        extras["serving"]["clocks"] = clk5.summary()
+        extras["serving"]["stream"] = ("96 requests, n log-uniform in [1e3, 1e5] (the full request stream of "
+                                       "4,096 requests up to 1e6 points runs with --serve)")
+
     if rank == 0:
         line = {
             "metric": "result pairs/s", "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": wl.dtype,
             "data": "synthetic (seeded Exp(40) generator, counter-based; no dataset is shipped)",
-            "config": {"workload": wl.name, "n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps,
-                       "refine": {1: "exact", 2: "tc_f16", 3: "tc_bf16"}.get(refine_used, str(refine_used)),
-                       "pairs_per_step": int(tot_pairs), "candidates_per_step": int(cand),
-                       "band_pairs": int(band), "tc_accepts": int(acc), "filter_delta": delta,
-                       "refine_kernel_ms": max_kern,
-                       "l2": "inputs larger than L2 (dataset 360 MB > 126 MB); no flush",
-                       "parallelism": f"query-block shards x{ws}" if ws > 1 else "single GPU"},
+            "config": workload_config(wl),
+            "run": {"refine": {1: "exact", 2: "tc_f16", 3: "tc_bf16"}.get(refine_used, str(refine_used)),
+                    "pairs_per_step": int(tot_pairs), "candidates_per_step": int(cand),
+                    "band_pairs": int(band), "tc_accepts": int(acc), "filter_delta": delta,
+                    "refine_kernel_ms": max_kern,
+                    "parallelism": f"query-block shards x{ws}" if ws > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk.summary(),
+            "clocks": clk.summary(), **extras,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

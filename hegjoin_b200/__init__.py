@@ -114,8 +114,6 @@ def _load() -> ctypes.CDLL:
         "hj_probe_tc_tile": (I, [P, I, U32, U32, P, P, P, P]),
         "hj_tc_operand_scale": (I, [P, P]),
         "hj_shard_plan": (I, [U32, U32, U32, P, P, P]),
-        "hj_generate_exp40": (I, [U64, U64, U64, U32, I, P]),
-        "hj_generate_skewed": (I, [U64, U64, U32, U32, D, D, I, P]),
         "hj_server_opts_default": (None, [P]),
         "hj_server_create": (I, [P, P]),
         "hj_server_submit": (I, [P, P, U32, U32, U32, I, D, P]),
@@ -376,19 +374,16 @@ def shard_plan(n_items: int, shard_count: int, shard_index: int):
 
 
 def generate_exp40(seed: int, n: int, d: int, dtype=np.float32, stream: int = 0) -> np.ndarray:
-    """Host generator (C++/OpenMP) producing the same values as workloads.exp40."""
-    out = np.empty((n, d), dtype=dtype)
-    check(lib.hj_generate_exp40(seed, stream, n, d, HJ_F32 if out.dtype == np.float32 else HJ_F64, out.ctypes.data))
-    return out
+    """Host generator (C++/OpenMP, libhj_datagen.so): the values of workloads.exp40."""
+    from . import workloads
+    return workloads.exp40(seed, n, d, dtype, stream)
 
 
 def generate_skewed(seed: int, n: int, d: int, n_clusters: int = 64, sigma: float = 0.002,
                     frac_clustered: float = 0.2, dtype=np.float32) -> np.ndarray:
     """Host generator of the skewed workload (80% Exp(40), 20% Gaussian clusters)."""
-    out = np.empty((n, d), dtype=dtype)
-    check(lib.hj_generate_skewed(seed, n, d, n_clusters, sigma, frac_clustered,
-                                 HJ_F32 if out.dtype == np.float32 else HJ_F64, out.ctypes.data))
-    return out
+    from . import workloads
+    return workloads.skewed(seed, n, d, n_clusters, sigma, frac_clustered, dtype)
 
 
 class _DeviceArray:

@@ -11,7 +11,7 @@
 #include <cmath>
 #include <cstdint>
 
-#include "hegjoin_b200.h"
+#include "hegjoin_datagen.h"
 
 namespace {
 constexpr uint64_t kSalt = 0xD1B54A32D192ED03ull;

@@ -5,7 +5,7 @@ that draws each coordinate i.i.d. from Exp(rate=40) with ``std::mt19937`` and
 redraws values above 1.  The workloads here keep that distribution but use a
 counter-based generator, so any slice of a dataset can be produced in parallel
 and reproduced bit for bit; its definition is hegjoin_b200/csrc/hj_datagen.cpp
-(host C++, reached through the library):
+(host C++, its own library libhj_datagen.so):
 
     u(seed, i, a) = (mix64(mix64(seed ^ SALT ^ K*stream) + 64*i + a) >> 11) * 2**-53   in [0, 1)
     x = -log1p(-u) / 40        (float64), cast to the dataset dtype,
@@ -20,21 +20,55 @@ query sample (stored to 17 significant digits in EPS_TABLE).
 """
 from __future__ import annotations
 
+import ctypes
 import dataclasses
+import os
 
 import numpy as np
 
+# The generator is its own host library (libhj_datagen.so, declared in
+# include/hegjoin_datagen.h): this module needs neither a GPU nor the join's
+# CUDA library, so a process timing a CPU join can make the same inputs.
+_DATAGEN_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libhj_datagen.so")
+_dg = None
+
+
+def _datagen():
+    global _dg
+    if _dg is None:
+        if not os.path.exists(_DATAGEN_PATH):
+            raise ImportError(f"{_DATAGEN_PATH} is missing: build it with `make -C hegjoin_b200/csrc`")
+        lib = ctypes.CDLL(_DATAGEN_PATH)
+        U32, U64, I, D, P = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+        lib.hj_generate_exp40.argtypes = [U64, U64, U64, U32, I, P]
+        lib.hj_generate_exp40.restype = I
+        lib.hj_generate_skewed.argtypes = [U64, U64, U32, U32, D, D, I, P]
+        lib.hj_generate_skewed.restype = I
+        _dg = lib
+    return _dg
+
+
+def _code(dtype) -> int:
+    return 0 if np.dtype(dtype) == np.float32 else 1
+
+
 def exp40(seed: int, n: int, d: int, dtype=np.float32, stream: int = 0) -> np.ndarray:
     """n x d coordinates, i.i.d. Exp(rate=40) redrawn into [0, 1) after the dtype cast."""
-    import hegjoin_b200 as hj
-    return hj.generate_exp40(seed, n, d, dtype, stream)
+    out = np.empty((n, d), dtype=dtype)
+    st = _datagen().hj_generate_exp40(seed, stream, n, d, _code(dtype), out.ctypes.data)
+    if st != 0:
+        raise ValueError(f"hj_generate_exp40 failed ({st})")
+    return out
 
 
 def skewed(seed: int, n: int, d: int, n_clusters: int = 64, sigma: float = 0.002,
            frac_clustered: float = 0.2, dtype=np.float32) -> np.ndarray:
     """80% Exp(40) points and 20% from Gaussian clusters, clipped to [0, 1)."""
-    import hegjoin_b200 as hj
-    return hj.generate_skewed(seed, n, d, n_clusters, sigma, frac_clustered, dtype)
+    out = np.empty((n, d), dtype=dtype)
+    st = _datagen().hj_generate_skewed(seed, n, d, n_clusters, sigma, frac_clustered, _code(dtype), out.ctypes.data)
+    if st != 0:
+        raise ValueError(f"hj_generate_skewed failed ({st})")
+    return out
 
 
 @dataclasses.dataclass(frozen=True)

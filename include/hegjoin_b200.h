@@ -248,17 +248,6 @@ hj_status hj_server_wait(hj_server* s, uint64_t ticket, double timeout_s, hj_res
                          hj_serve_info* info);
 hj_status hj_server_destroy(hj_server* s);
 
-/* ---- synthetic data ---------------------------------------------------------- */
-/* n x d coordinates i.i.d. Exp(rate=40), redrawn into [0, 1) after the cast to
- * the dataset type, from a counter-based generator (seed, stream): the same
- * values hegjoin_b200.workloads.exp40 produces.  Host memory; OpenMP. */
-hj_status hj_generate_exp40(uint64_t seed, uint64_t stream, uint64_t n, uint32_t d, int dtype, void* h_out);
-/* The skewed workload: the first n - round(frac * n) points from
- * hj_generate_exp40(seed, 0, ...), the rest from n_clusters Gaussian clusters
- * (standard deviation sigma, centres uniform in [0,1)^d), clipped to [0, 1). */
-hj_status hj_generate_skewed(uint64_t seed, uint64_t n, uint32_t d, uint32_t n_clusters, double sigma,
-                             double frac_clustered, int dtype, void* h_out);
-
 /* ---- probes --------------------------------------------------------------- */
 /* Evaluates the reference's squared-distance expression (kernel.cu:350-353)
  * as nvcc compiles it by default, for n pairs of d-dimensional rows; writes

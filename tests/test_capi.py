@@ -6,25 +6,30 @@ import re
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def _declared():
-    names = set()
-    for fn in os.listdir(os.path.join(ROOT, "include")):
-        if not fn.endswith(".h"):
-            continue
-        src = open(os.path.join(ROOT, "include", fn)).read()
-        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        for m in re.finditer(r"\b(hj_\w+)\s*\(", src):
-            names.add(m.group(1))
-    return names
+# header -> the library that must export every hj_* function it declares
+LIBS = {"hegjoin_b200.h": "libhegjoin_b200.so", "hegjoin_datagen.h": "libhj_datagen.so"}
+
+
+def _declared(header):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return {m.group(1) for m in re.finditer(r"\b(hj_\w+)\s*\(", src)}
 
 
 def test_library_exports_declared_symbols():
-    import hegjoin_b200
-    lib = ctypes.CDLL(hegjoin_b200.LIB_PATH)
-    declared = _declared()
-    assert "hj_join" in declared and "hj_index_create" in declared
-    missing = [n for n in sorted(declared) if not hasattr(lib, n)]
-    assert not missing, missing
+    import hegjoin_b200  # noqa: F401  (the package loads its library)
+    for header, libname in LIBS.items():
+        lib = ctypes.CDLL(os.path.join(ROOT, "hegjoin_b200", libname))
+        declared = _declared(header)
+        assert declared, header
+        missing = [n for n in sorted(declared) if not hasattr(lib, n)]
+        assert not missing, (header, missing)
+    assert {"hj_join", "hj_index_create"} <= _declared("hegjoin_b200.h")
+
+
+def test_join_library_does_not_carry_the_generator():
+    lib = ctypes.CDLL(os.path.join(ROOT, "hegjoin_b200", "libhegjoin_b200.so"))
+    assert not hasattr(lib, "hj_generate_exp40")
 
 
 def test_version_and_error_without_gpu():
