@@ -175,11 +175,52 @@ def load_workloads():
     return mod
 
 
+L2_BYTES = 126 * 1000 * 1000
+
+
+def dataset_bytes(wl) -> int:
+    return wl.n * wl.d * (4 if wl.dtype == "f32" else 8)
+
+
 def workload_config(wl):
     """The `config` both arms print for a workload (identical keys and values)."""
+    mb = dataset_bytes(wl) / 1e6
+    l2 = (f"inputs larger than L2 ({mb:.0f} MB dataset > 126 MB L2); no flush" if dataset_bytes(wl) > L2_BYTES else
+          f"dataset ({mb:.0f} MB) fits in L2: a 512 MB buffer is written between timed steps (untimed)")
     return {"workload": wl.name, "n": wl.n, "d": wl.d, "k": wl.k, "eps": wl.eps, "dtype": wl.dtype,
-            "seed": wl.seed, "l2": f"inputs larger than L2 ({wl.n * wl.d * (4 if wl.dtype == 'f32' else 8) / 1e6:.0f} "
-                                  f"MB dataset > 126 MB L2); no flush"}
+            "seed": wl.seed, "l2": l2}
+
+
+class HostRing:
+    """A batch sink that reads every result pair on the host: each batch's
+    neighbour ids are copied, in chunks, into a ring of two pinned host buffers
+    on the join's stream (a chunk's buffer is reused once its previous copy is done)."""
+
+    def __init__(self, chunk_elems: int = 1 << 28):
+        import torch
+        self.torch = torch
+        self.bufs = [torch.empty(chunk_elems, dtype=torch.int32).pin_memory() for _ in range(2)]
+        self.events = [torch.cuda.Event() for _ in range(2)]
+        self.used = [False, False]
+        self.chunk = chunk_elems
+        self.bytes = 0
+        self.i = 0
+
+    def __call__(self, batch, count, keys, vals, stream):
+        import hegjoin_b200 as hj
+        src = hj.device_view(vals, (count,), np.int32)
+        for off in range(0, count, self.chunk):
+            m = min(self.chunk, count - off)
+            slot = self.i % 2
+            if self.used[slot]:
+                self.events[slot].synchronize()
+            self.bufs[slot][:m].copy_(src[off:off + m], non_blocking=True)
+            self.events[slot].record()
+            self.used[slot] = True
+            self.i += 1
+        self.bytes += 4 * count
+        return 0
+
 
 
 def reference_arm(args, wl):
@@ -358,8 +399,8 @@ def tc_vs_plain(wl, steps: int, warmup: int, tc_kind: str = "auto"):
         out[refine] = {"pairs": int(st.total_pairs), "seconds_per_step": sec, "pairs_per_s": st.total_pairs / sec,
                        "refine_used": {1: "exact", 2: "tc_f16", 3: "tc_bf16"}.get(int(st.refine_used)),
                        "refine_kernel_ms": st.ms_refine_kernel,
-                       "join_ms": {"estimate": st.ms_estimate, "refine": st.ms_refine, "group": st.ms_group,
-                                   "total": st.ms_total},
+                       "join_ms": {"setup": st.ms_setup, "estimate": st.ms_estimate, "refine": st.ms_refine,
+                                   "group": st.ms_group, "total": st.ms_total},
                        "batches": int(st.n_batches), "retries": int(st.n_retries), "band_pairs": int(st.band_pairs),
                        "tc_accepts": int(st.tc_accepts), "filter_delta": st.filter_delta,
                        "candidates": int(cand)}
@@ -407,6 +448,45 @@ def compare_bench(args, wl):
           flush=True)
 
 
+# ---------------------------------------------------------------------------------------------
+# dataset ingest at the skewed 6-D configuration's size: --ingest
+def ingest_bench(args, wl):
+    """The reference's text importer (import_dataset.cpp:10-40, restated in the oracle
+    with the same stringstream calls, one thread) against hj_import_text (all host
+    threads) and the binary twin, on the workload written in the reference
+    generator's layout with max_digits10 significant digits."""
+    import tempfile
+    import hegjoin_b200 as hj
+    import oracle
+    db = wl.generate()
+    digits = 9 if db.dtype == np.float32 else 17
+    with tempfile.TemporaryDirectory() as tmp:
+        txt, binp = os.path.join(tmp, "db.txt"), os.path.join(tmp, "db.hjds")
+        oracle.write_text(txt, db, digits)
+        size = os.path.getsize(txt)
+        times = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            got = hj.import_text(txt, wl.d, db.dtype)
+            times.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        ref = oracle.import_text(txt, db.dtype)
+        t_ref = time.perf_counter() - t0
+        same = bool(np.array_equal(got.reshape(-1).view(np.uint8), ref.view(np.uint8))) and np.array_equal(got, db)
+        hj.write_binary(binp, db)
+        t0 = time.perf_counter()
+        gb = hj.import_binary(binp, wl.d, db.dtype)
+        t_bin = time.perf_counter() - t0
+    print(json.dumps({"metric": "dataset ingest (values/s)", "workload": wl.name, "n": wl.n, "d": wl.d,
+                      "text_bytes": size, "values": int(db.size), "identical_values": same,
+                      "binary_identical": bool(np.array_equal(gb, db)),
+                      "reference_stringstream": {"seconds": t_ref, "values_per_s": db.size / t_ref, "threads": 1},
+                      "hj_import_text": {"seconds": min(times), "values_per_s": db.size / min(times),
+                                         "threads": os.cpu_count()},
+                      "hj_import_binary": {"seconds": t_bin, "values_per_s": db.size / t_bin},
+                      "speedup_text": t_ref / min(times)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -418,6 +498,8 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="override the workload's point count (testing only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--stream", action="store_true",
+                    help="consume each batch instead of keeping the result (default for c1_2d)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the tensor-core-vs-plain (90-D) and serving blocks of the default line")
     ap.add_argument("--extra-steps", type=int, default=2)
@@ -433,6 +515,7 @@ def main():
     ap.add_argument("--serve-seed", type=int, default=5)
     ap.add_argument("--compare", action="store_true", help="time the exact refine against the tensor-core filter")
     ap.add_argument("--tc-kind", default="auto", choices=["auto", "tc_f16", "tc_bf16"])
+    ap.add_argument("--ingest", action="store_true", help="time the text importer against the reference's")
     args = ap.parse_args()
     if args.serve:
         serve_bench(args)
@@ -449,6 +532,9 @@ def main():
     if args.compare:
         compare_bench(args, wl)
         return
+    if args.ingest:
+        ingest_bench(args, wl)
+        return
 
     import torch
     import torch.distributed as dist
@@ -461,14 +547,26 @@ def main():
     stream = torch.cuda.current_stream(dev)
     shard = dict(shard_count=ws, shard_index=rank) if ws > 1 else {}
 
+    # results too large to keep on the device (the 2-D, 2M-point configuration: ~1.9e10
+    # pairs, 76 GB of neighbour ids) go through the streamed join: each grouped batch is
+    # consumed (per-query digests on the device) and its buffers reused
+    stream_mode = args.stream or wl.name == "c1_2d"
+    flush = torch.empty(512 * 1000 * 1000 // 4, dtype=torch.float32, device=dev) \
+        if dataset_bytes(wl) <= L2_BYTES else None
+
     def one_step():
         ix = hj.GridIndex(db, wl.k, wl.eps)
         cand = ix.sort_by_workload()
-        res = hj.join(ix, refine=args.refine, **shard)
-        st = res.stats
-        out = (res.total_pairs, cand, st.ms_refine_kernel, st.refine_launches, st.refine_used, st.band_pairs,
-               st.tc_accepts, st.filter_delta)
-        res.close()
+        if stream_mode:
+            st, _ = hj.join_stream(ix, None, digest=True, refine=args.refine, **shard)
+            pairs = st.total_pairs
+        else:
+            res = hj.join(ix, refine=args.refine, **shard)
+            st = res.stats
+            pairs = res.total_pairs
+            res.close()
+        out = (pairs, cand, st.ms_refine_kernel, st.refine_launches, st.refine_used, st.band_pairs,
+               st.tc_accepts, st.filter_delta, int(st.n_batches))
         ix.close()
         return out
 
@@ -478,18 +576,30 @@ def main():
     barrier()
     torch.cuda.synchronize()
     launches0 = hj.kernel_launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     recs = []
+    ms = 0.0
     with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            recs.append(one_step())
-        e1.record(stream)
-        torch.cuda.synchronize()
+        if flush is None:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                recs.append(one_step())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+        else:
+            # the dataset fits in L2: write a larger buffer before every step, outside the timing
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                recs.append(one_step())
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
     barrier()
     torch.cuda.synchronize()
     launches = hj.kernel_launch_count() - launches0
-    ms = e0.elapsed_time(e1)
     ms_step = ms / args.steps
     pairs = recs[-1][0]
     cand = recs[-1][1]
@@ -535,7 +645,39 @@ def main():
 
     # end to end through the host entry point: pinned H2D in, full result D2H out
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and stream_mode:
+        # streamed: pinned H2D of the dataset, the join, and every batch's neighbour ids
+        # plus the per-query counts copied back to pinned host memory
+        host_db = torch.from_numpy(np_db).pin_memory()
+        ring = HostRing()
+        e2e_ms, d2h = [], 0
+        cnt_h = torch.empty(np_db.shape[0], dtype=torch.int32).pin_memory()
+        for it in range(1 + args.steps):
+            if flush is not None:
+                flush.fill_(1.0)
+            torch.cuda.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            ring.bytes = 0
+            d_db = host_db.to(dev, non_blocking=True)
+            ix = hj.GridIndex(d_db, wl.k, wl.eps)
+            ix.sort_by_workload()
+            st, (c, _, _) = hj.join_stream(ix, ring, digest=True, refine=args.refine, **shard)
+            cnt_h.copy_(c, non_blocking=True)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            ix.close()
+            del d_db
+            d2h = ring.bytes + cnt_h.numel() * 4
+            if it >= 1:
+                e2e_ms.append((t1 - t0) * 1e3)
+        e_ms = statistics.mean(e2e_ms)
+        e_ms_max, = allreduce([e_ms], dist.ReduceOp.MAX) if ws > 1 else [e_ms]
+        e2e = {"value": tot_pairs / (e_ms_max / 1e3), "unit": "pairs/s",
+               "h2d_bytes_per_step": int(np_db.nbytes), "d2h_bytes_per_step": int(d2h), "ms_per_step": e_ms_max,
+               "path": "pinned H2D, GridIndex + join_stream; each batch's neighbour ids and the per-query "
+                       "counts copied to pinned host memory"}
+    elif not args.no_e2e:
         host_db = torch.from_numpy(np_db).pin_memory()
         n = np_db.shape[0]
         off_h = torch.empty(n + 1, dtype=torch.int64).pin_memory()
@@ -578,7 +720,7 @@ def main():
 
     # the north-star comparisons, each with its own clock record (single GPU only)
     extras = {}
-    if ws == 1 and not args.no_extras:
+    if ws == 1 and not args.no_extras and wl.name == "c2_18d":
         del db
         torch.cuda.empty_cache()
         with ClockSampler(local) as clk3:
@@ -600,7 +742,9 @@ def main():
             "run": {"refine": {1: "exact", 2: "tc_f16", 3: "tc_bf16"}.get(refine_used, str(refine_used)),
                     "pairs_per_step": int(tot_pairs), "candidates_per_step": int(cand),
                     "band_pairs": int(band), "tc_accepts": int(acc), "filter_delta": delta,
-                    "refine_kernel_ms": max_kern,
+                    "refine_kernel_ms": max_kern, "batches": int(recs[-1][8]),
+                    "result": "streamed: per-query digests on the device, batches not kept" if stream_mode else
+                              "kept on the device (per-batch neighbour ids + neighbour table)",
                     "parallelism": f"query-block shards x{ws}" if ws > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(), **extras,

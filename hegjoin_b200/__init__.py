@@ -68,10 +68,19 @@ class JoinStats(ctypes.Structure):
                 ("filter_delta", ctypes.c_double), ("ms_estimate", ctypes.c_float), ("ms_refine", ctypes.c_float),
                 ("ms_group", ctypes.c_float), ("ms_total", ctypes.c_float), ("ms_refine_kernel", ctypes.c_float),
                 ("refine_launches", ctypes.c_uint32), ("refine_used", ctypes.c_uint32),
-                ("kernel_launches", ctypes.c_uint32)]
+                ("kernel_launches", ctypes.c_uint32), ("ms_setup", ctypes.c_float)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class BatchView(ctypes.Structure):
+    _fields_ = [("batch", ctypes.c_uint32), ("pad_", ctypes.c_uint32), ("count", ctypes.c_uint64),
+                ("d_keys", ctypes.c_void_p), ("d_vals", ctypes.c_void_p)]
+
+
+# hj_batch_sink: hj_status (*)(const hj_batch_view*, void* user, void* stream)
+BATCH_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(BatchView), ctypes.c_void_p, ctypes.c_void_p)
 
 
 class ServerOpts(ctypes.Structure):
@@ -113,7 +122,16 @@ def _load() -> ctypes.CDLL:
         "hj_probe_sqdist": (I, [P, P, U32, U32, I, P, P]),
         "hj_probe_tc_tile": (I, [P, I, U32, U32, P, P, P, P]),
         "hj_tc_operand_scale": (I, [P, P]),
+        "hj_probe_tc_wait_timeout": (I, [P, I, U64, P]),
         "hj_shard_plan": (I, [U32, U32, U32, P, P, P]),
+        "hj_shard_plan_lpt": (I, [P, U32, U32, U32, P, P]),
+        "hj_join_stream": (I, [P, P, BATCH_SINK, P, P, P, P, P, P]),
+        "hj_debug_fail_alloc": (None, [U64]),
+        "hj_debug_pool_used": (I, [P]),
+        "hj_import_text": (I, [ctypes.c_char_p, U32, I, P, P]),
+        "hj_import_binary": (I, [ctypes.c_char_p, U32, I, P, P]),
+        "hj_write_binary": (I, [ctypes.c_char_p, P, U64, U32, I]),
+        "hj_host_free": (None, [P]),
         "hj_server_opts_default": (None, [P]),
         "hj_server_create": (I, [P, P]),
         "hj_server_submit": (I, [P, P, U32, U32, U32, I, D, P]),
@@ -331,6 +349,62 @@ def join(index: GridIndex, stream=None, **kw) -> JoinResult:
     return JoinResult(h, st, index.info().n, index.db.device)
 
 
+def join_stream(index: GridIndex, sink=None, digest: bool = True, stream=None, **kw):
+    """The join with nothing kept on the device (hj_join_stream): every grouped batch
+    goes to `sink(batch, count, keys_ptr, vals_ptr, stream_ptr)` (device pointers,
+    valid for work enqueued on that stream) and per-query digests accumulate on the
+    device.  Returns (JoinStats, (count, sum, xor) CUDA tensors or None)."""
+    torch = _torch()
+    n = index.info().n
+    dev = index.db.device
+    cnt = s = x = None
+    if digest:
+        cnt = torch.empty(n, dtype=torch.int32, device=dev)
+        s = torch.empty(n, dtype=torch.int64, device=dev)
+        x = torch.empty(n, dtype=torch.int64, device=dev)
+    errors = []
+
+    def _cb(view, user, st):
+        try:
+            v = view.contents
+            r = sink(int(v.batch), int(v.count), v.d_keys, v.d_vals, st)
+            return HJ_OK if r is None else int(r)
+        except Exception as e:          # a Python error stops the join with a clear status
+            errors.append(e)
+            return HJ_ERR_INVALID
+
+    cb = BATCH_SINK(_cb) if sink is not None else BATCH_SINK()
+    o = join_opts(**kw)
+    st = JoinStats()
+    status = lib.hj_join_stream(index.handle, ctypes.byref(o), cb, None, _ptr(cnt) if digest else None,
+                                _ptr(s) if digest else None, _ptr(x) if digest else None, _stream_ptr(stream),
+                                ctypes.byref(st))
+    if errors:
+        raise errors[0]
+    check(status)
+    return st, ((cnt, s, x) if digest else None)
+
+
+def shard_plan_lpt(costs, shard_count: int, shard_index: int) -> np.ndarray:
+    """Item indices (ascending) that rank `shard_index` takes under greedy LPT."""
+    c = np.ascontiguousarray(costs, dtype=np.uint64)
+    items = np.zeros(max(1, len(c)), np.uint32)
+    m = ctypes.c_uint32()
+    check(lib.hj_shard_plan_lpt(c.ctypes.data, len(c), shard_count, shard_index, items.ctypes.data, ctypes.byref(m)))
+    return items[:m.value]
+
+
+def debug_fail_alloc(nth: int) -> None:
+    """Make the nth device allocation from now fail as an out-of-memory would (0 disarms)."""
+    lib.hj_debug_fail_alloc(int(nth))
+
+
+def debug_pool_used() -> int:
+    b = ctypes.c_uint64()
+    check(lib.hj_debug_pool_used(ctypes.byref(b)))
+    return int(b.value)
+
+
 def self_join_host(db: np.ndarray, k: int, eps: float, stream=None, keep=True, **kw):
     """One-shot join from host memory (copies in, index, workload order, join)."""
     db = np.ascontiguousarray(db)
@@ -371,6 +445,39 @@ def shard_plan(n_items: int, shard_count: int, shard_index: int):
     f, s, m = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
     check(lib.hj_shard_plan(n_items, shard_count, shard_index, ctypes.byref(f), ctypes.byref(s), ctypes.byref(m)))
     return f.value, s.value, m.value
+
+
+def _take_host(ptr: ctypes.c_void_p, n: int, d: int, dtype) -> np.ndarray:
+    """Copy a library-allocated n x d host array into numpy and release it."""
+    try:
+        if n == 0:
+            return np.zeros((0, d), dtype=dtype)
+        buf = (ctypes.c_char * (n * d * np.dtype(dtype).itemsize)).from_address(ptr.value)
+        return np.frombuffer(buf, dtype=dtype).reshape(n, d).copy()
+    finally:
+        lib.hj_host_free(ptr)
+
+
+def import_text(path: str, d: int, dtype=np.float32) -> np.ndarray:
+    """importNDDataset (import_dataset.cpp:10-40): the reference's text format, parsed in parallel."""
+    out, n = ctypes.c_void_p(), ctypes.c_uint64()
+    check(lib.hj_import_text(os.fsencode(path), d, HJ_F32 if np.dtype(dtype) == np.float32 else HJ_F64,
+                             ctypes.byref(out), ctypes.byref(n)))
+    return _take_host(out, n.value, d, dtype)
+
+
+def import_binary(path: str, d: int, dtype=np.float32) -> np.ndarray:
+    """The binary twin (or the reference's raw binary layout)."""
+    out, n = ctypes.c_void_p(), ctypes.c_uint64()
+    check(lib.hj_import_binary(os.fsencode(path), d, HJ_F32 if np.dtype(dtype) == np.float32 else HJ_F64,
+                               ctypes.byref(out), ctypes.byref(n)))
+    return _take_host(out, n.value, d, dtype)
+
+
+def write_binary(path: str, db: np.ndarray) -> None:
+    db = np.ascontiguousarray(db)
+    check(lib.hj_write_binary(os.fsencode(path), db.ctypes.data, db.shape[0], db.shape[1],
+                              HJ_F32 if db.dtype == np.float32 else HJ_F64))
 
 
 def generate_exp40(seed: int, n: int, d: int, dtype=np.float32, stream: int = 0) -> np.ndarray:

@@ -172,39 +172,54 @@ void distanceTableNDGridBatches(int searchMode, float staticPartition, unsigned 
     const unsigned n = *DBSIZE;
     hj_join_opts o;
     hj_join_opts_default(&o);
-    hj_result* r = nullptr;
+    // Each grouped batch comes to the host as it completes (GPU.cu:1542-1573): keys and
+    // values through pinned staging, then a new int[] of values per batch and the
+    // neighbour-table entries pointing into it.  Nothing stays on the device, so the
+    // result may exceed device memory, as in the reference.
+    struct Sink {
+        neighborTableLookup* table;
+        std::vector<neighborDataPtrs>* ptrs;
+        int* keys = nullptr;
+        int* vals = nullptr;
+        uint64_t cap = 0;
+        ~Sink() {
+            if (keys) cudaFreeHost(keys);
+            if (vals) cudaFreeHost(vals);
+        }
+        static hj_status on_batch(const hj_batch_view* b, void* user, void* stream) {
+            Sink* S = static_cast<Sink*>(user);
+            if (b->count == 0) return HJ_OK;
+            if (b->count > 0x7FFFFFFFull) return HJ_ERR_OVERFLOW;   // the table stores int offsets
+            cudaStream_t st = static_cast<cudaStream_t>(stream);
+            if (b->count > S->cap) {
+                if (S->keys) cudaFreeHost(S->keys);
+                if (S->vals) cudaFreeHost(S->vals);
+                S->keys = S->vals = nullptr;
+                S->cap = 0;
+                if (cudaMallocHost((void**)&S->keys, b->count * sizeof(int)) != cudaSuccess ||
+                    cudaMallocHost((void**)&S->vals, b->count * sizeof(int)) != cudaSuccess)
+                    return HJ_ERR_OOM;
+                S->cap = b->count;
+            }
+            if (cudaMemcpyAsync(S->keys, b->d_keys, b->count * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaMemcpyAsync(S->vals, b->d_vals, b->count * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return HJ_ERR_CUDA;
+            unsigned cnt = (unsigned)b->count;
+            int* kept = new int[cnt];   // owned by pointersToNeighbors, as in the reference
+            constructNeighborTableKeyValueWithPtrs(S->keys, S->vals, S->table, kept, &cnt);
+            S->ptrs->push_back(neighborDataPtrs{kept, (int)cnt});
+            return HJ_OK;
+        }
+    } sink;
+    sink.table = neighborTable;
+    sink.ptrs = pointersToNeighbors;
     hj_join_stats st;
-    if (!report(T, hj_join(ix, &o, nullptr, &r, &st))) return;
+    if (!report(T, hj_join_stream(ix, &o, &Sink::on_batch, &sink, nullptr, nullptr, nullptr, nullptr, &st))) return;
     if (setQueueIndex) setQueueIndex(n);   // all queries went to the GPU
-    uint32_t nb = 0;
-    uint64_t total = 0;
-    hj_result_num_batches(r, &nb, &total);
-    std::vector<int*> batch_ptr(nb, nullptr);
-    for (uint32_t b = 0; b < nb; ++b) {
-        const uint32_t* dv = nullptr;
-        uint64_t cnt = 0;
-        hj_result_batch(r, b, &dv, nullptr, &cnt);
-        int* hv = new int[cnt ? cnt : 1];
-        if (cnt) report_cuda(T, "cudaMemcpy", cudaMemcpy(hv, dv, cnt * sizeof(int), cudaMemcpyDeviceToHost));
-        batch_ptr[b] = hv;
-        pointersToNeighbors->push_back(neighborDataPtrs{hv, (int)cnt});
-    }
-    const hj_nt_entry* dt = nullptr;
-    hj_result_table(r, &dt);
-    std::vector<hj_nt_entry> table(n);
-    report_cuda(T, "cudaMemcpy", cudaMemcpy(table.data(), dt, sizeof(hj_nt_entry) * n, cudaMemcpyDeviceToHost));
-    for (unsigned q = 0; q < n; ++q) {
-        const hj_nt_entry& e = table[q];
-        if (!e.count) continue;
-        neighborTable[q].pointID = (int)q;
-        neighborTable[q].indexmin = (int)e.start;
-        neighborTable[q].indexmax = (int)(e.start + e.count);
-        neighborTable[q].dataPtr = batch_ptr[e.batch];
-    }
-    hj_result_destroy(r);
-    *totalNeighbors = total;
+    *totalNeighbors = st.total_pairs;
     *nbQueriesGPU = n;
-    printf("[GPU] ~ Total result set size on host: %llu\n", (unsigned long long)total);
+    printf("[GPU] ~ Total result set size on host: %llu\n", (unsigned long long)st.total_pairs);
 }
 
 void constructNeighborTableKeyValueWithPtrs(int* pointIDKey, int* pointInDistValue,

@@ -67,11 +67,19 @@ inline hj_status launch_status(const char* file, int line) {
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ---- device buffers ----------------------------------------------------------
+// Fault injection for tests (hj_debug_fail_alloc): while armed with n > 0, the
+// n-th dalloc from then on fails the way an out-of-memory would.
+bool injected_alloc_failure();   // hj_index.cu
+
 // Stream-ordered device allocation; freed with dfree on the same stream.
 template <typename T>
 hj_status dalloc(T** p, size_t count, cudaStream_t st) {
     *p = nullptr;
     if (count == 0) count = 1;
+    if (injected_alloc_failure()) {
+        set_error("device allocation of %zu bytes failed: injected failure", count * sizeof(T));
+        return HJ_ERR_OOM;
+    }
     cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), count * sizeof(T), st);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -86,6 +94,55 @@ void dfree(T*& p, cudaStream_t st) {
     if (p) cudaFreeAsync(p, st);
     p = nullptr;
 }
+
+// The device temporaries of one call: everything allocated through the guard is
+// freed (in the order of its stream) when the guard goes out of scope, on every
+// return path, unless it was handed over with keep().
+class Scratch {
+  public:
+    explicit Scratch(cudaStream_t st) : st_(st) {}
+    Scratch(const Scratch&) = delete;
+    Scratch& operator=(const Scratch&) = delete;
+    ~Scratch() {
+        for (void* p : held_) cudaFreeAsync(p, st_);
+    }
+    template <typename T>
+    hj_status alloc(T** p, size_t count) {
+        hj_status s = dalloc(p, count, st_);
+        if (s == HJ_OK) held_.push_back(*p);
+        return s;
+    }
+    // Free one temporary now (its memory goes back to the pool for the next allocation).
+    template <typename T>
+    void release(T*& p) {
+        drop(p);
+        dfree(p, st_);
+    }
+    // Hand a buffer to a longer-lived owner: the guard no longer frees it.
+    template <typename T>
+    T* keep(T* p) {
+        drop(p);
+        return p;
+    }
+    // Take charge of a buffer allocated elsewhere (freed with the others).
+    template <typename T>
+    T* adopt(T* p) {
+        if (p) held_.push_back(p);
+        return p;
+    }
+
+  private:
+    void drop(const void* p) {
+        for (size_t i = 0; i < held_.size(); ++i)
+            if (held_[i] == p) {
+                held_[i] = held_.back();
+                held_.pop_back();
+                return;
+            }
+    }
+    cudaStream_t st_;
+    std::vector<void*> held_;
+};
 
 // Raise a kernel's dynamic shared-memory limit once per (kernel, size), safe
 // when several host threads launch joins concurrently.

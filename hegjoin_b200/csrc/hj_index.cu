@@ -43,6 +43,12 @@ void count_launch() {
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 uint64_t thread_launch_count() { return t_launches; }
 
+static std::atomic<int64_t> g_fail_alloc_in{0};
+bool injected_alloc_failure() {
+    if (g_fail_alloc_in.load(std::memory_order_relaxed) <= 0) return false;
+    return g_fail_alloc_in.fetch_sub(1, std::memory_order_relaxed) == 1;
+}
+
 hj_status ensure_smem_ptr(const void* kern, size_t bytes) {
     static std::mutex mu;
     static std::map<const void*, size_t> done;
@@ -67,6 +73,12 @@ void init_memory_pool() {
     if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
         uint64_t keep = ~0ull;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        // Concurrent joins (the serving loop's workers) allocate and free on their own
+        // streams.  By default the pool may hand one stream memory another stream freed
+        // by making the allocation wait for that stream, which couples the requests;
+        // reuse only memory whose free has completed, or that was freed on the same stream.
+        int no = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
     }
     cudaGetLastError();
 }
@@ -135,8 +147,9 @@ template <typename T>
 hj_status geometry_t(const T* db, uint32_t n, uint32_t d, uint32_t k, T eps, double* h_min, double* h_max,
                      uint32_t* h_ncells, uint64_t* h_total, cudaStream_t st) {
     const int blocks = std::min<int>(num_sms() * 4, std::max<uint32_t>(1, (n + 255) / 256));
+    Scratch tmp(st);
     T* part = nullptr;
-    HJ_TRY(dalloc(&part, (size_t)2 * blocks * k, st));
+    HJ_TRY(tmp.alloc(&part, (size_t)2 * blocks * k));
     for (uint32_t j = 0; j < k; ++j) {
         k_minmax<T><<<blocks, 256, 0, st>>>(db, n, d, j, part + (size_t)j * blocks, part + (size_t)(k + j) * blocks);
         HJ_LAUNCHED();
@@ -144,7 +157,6 @@ hj_status geometry_t(const T* db, uint32_t n, uint32_t d, uint32_t k, T eps, dou
     std::vector<T> hp((size_t)2 * blocks * k);
     HJ_CUDA(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(T), cudaMemcpyDeviceToHost, st));
     HJ_CUDA(cudaStreamSynchronize(st));
-    dfree(part, st);
     uint64_t total = 1;
     for (uint32_t j = 0; j < k; ++j) {
         T mn = hp[(size_t)j * blocks], mx = hp[(size_t)(k + j) * blocks];
@@ -353,13 +365,15 @@ hj_status index_create_t(const T* d_db, uint32_t n, uint32_t d, uint32_t k, T ep
         mul *= h_ncells[j];
         ix->total_cells *= h_ncells[j];
     }
+    // temporaries: freed on every return path; the index's own arrays are freed by free_index on failure
+    Scratch tmp(st);
     unsigned long long *keys = nullptr, *keys_tmp = nullptr;
     uint32_t *vals_tmp = nullptr, *flags = nullptr, *pos = nullptr, *scalars = nullptr;
-    HJ_TRY(dalloc(&keys, n, st));
-    HJ_TRY(dalloc(&keys_tmp, n, st));
+    HJ_TRY(tmp.alloc(&keys, n));
+    HJ_TRY(tmp.alloc(&keys_tmp, n));
     HJ_TRY(dalloc(&ix->perm, n, st));
-    HJ_TRY(dalloc(&vals_tmp, n, st));
-    HJ_TRY(dalloc(&scalars, 4, st));
+    HJ_TRY(tmp.alloc(&vals_tmp, n));
+    HJ_TRY(tmp.alloc(&scalars, 4));
     HJ_CUDA(cudaMemsetAsync(scalars, 0, 4 * sizeof(uint32_t), st));
     unsigned grid1 = (n + 255) / 256;
     k_cell_ids<T><<<grid1, 256, 0, st>>>(d_db, n, d, geo, ix->grid, keys, ix->perm, scalars);
@@ -367,10 +381,10 @@ hj_status index_create_t(const T* d_db, uint32_t n, uint32_t d, uint32_t k, T ep
     uint32_t nbits = bits_for(ix->total_cells > 0 ? ix->total_cells - 1 : 0);
     HJ_TRY(radix_sort_u64_u32(reinterpret_cast<uint64_t*>(keys), ix->perm, reinterpret_cast<uint64_t*>(keys_tmp),
                               vals_tmp, n, nbits, st));
-    dfree(keys_tmp, st);
-    dfree(vals_tmp, st);
-    HJ_TRY(dalloc(&flags, n, st));
-    HJ_TRY(dalloc(&pos, n, st));
+    tmp.release(keys_tmp);
+    tmp.release(vals_tmp);
+    HJ_TRY(tmp.alloc(&flags, n));
+    HJ_TRY(tmp.alloc(&pos, n));
     k_run_flags<<<grid1, 256, 0, st>>>(keys, n, flags);
     HJ_LAUNCHED();
     HJ_CUDA(cudaMemcpyAsync(pos, flags, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
@@ -390,10 +404,6 @@ hj_status index_create_t(const T* d_db, uint32_t n, uint32_t d, uint32_t k, T ep
     HJ_CUDA(cudaStreamSynchronize(st));
     ix->aliasing = hs[0];
     ix->nC = hs[1];
-    dfree(keys, st);
-    dfree(flags, st);
-    dfree(pos, st);
-    dfree(scalars, st);
     if (ix->aliasing) {
         set_error("grid aliasing: a point's cell coordinate reaches nCells in some indexed dimension "
                   "(epsilon below the coordinates' rounding granularity); unsupported");
@@ -454,8 +464,9 @@ void free_index(hj_index* ix, cudaStream_t st) {
 
 hj_status build_blocks(const hj_index* ix, uint32_t qb, HjBlock** d_blocks, uint32_t* n_blocks, cudaStream_t st) {
     uint32_t nC = ix->nC;
+    Scratch tmp(st);
     uint32_t* cnt = nullptr;
-    HJ_TRY(dalloc(&cnt, (size_t)nC + 1, st));
+    HJ_TRY(tmp.alloc(&cnt, (size_t)nC + 1));
     unsigned g = (nC + 255) / 256;
     k_block_counts<<<g, 256, 0, st>>>(ix->cell_order, ix->cell_start, nC, qb, cnt);
     HJ_LAUNCHED();
@@ -464,10 +475,11 @@ hj_status build_blocks(const hj_index* ix, uint32_t qb, HjBlock** d_blocks, uint
     uint32_t nb = 0;
     HJ_CUDA(cudaMemcpyAsync(&nb, cnt + nC, 4, cudaMemcpyDeviceToHost, st));
     HJ_CUDA(cudaStreamSynchronize(st));
-    HJ_TRY(dalloc(d_blocks, (size_t)std::max<uint32_t>(nb, 1), st));
-    k_make_blocks<<<g, 256, 0, st>>>(ix->cell_order, ix->cell_start, ix->cell_nb, cnt, nC, qb, *d_blocks);
+    HjBlock* blocks = nullptr;
+    HJ_TRY(tmp.alloc(&blocks, (size_t)std::max<uint32_t>(nb, 1)));
+    k_make_blocks<<<g, 256, 0, st>>>(ix->cell_order, ix->cell_start, ix->cell_nb, cnt, nC, qb, blocks);
     HJ_LAUNCHED();
-    dfree(cnt, st);
+    *d_blocks = tmp.keep(blocks);
     *n_blocks = nb;
     return HJ_OK;
 }
@@ -479,6 +491,20 @@ using namespace hj;
 extern "C" {
 
 const char* hj_last_error(void) { return hj::g_err; }
+
+void hj_debug_fail_alloc(uint64_t nth) { hj::g_fail_alloc_in.store((int64_t)nth, std::memory_order_relaxed); }
+
+hj_status hj_debug_pool_used(uint64_t* bytes) {
+    if (!bytes) { set_error("hj_debug_pool_used: null argument"); return HJ_ERR_INVALID; }
+    int dev = 0;
+    cudaMemPool_t pool;
+    HJ_CUDA(cudaGetDevice(&dev));
+    HJ_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    unsigned long long used = 0;   // cudaMemPoolAttrUsedMemCurrent is a 64-bit count
+    HJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    *bytes = (uint64_t)used;
+    return HJ_OK;
+}
 const char* hj_version(void) { return "hegjoin_b200 0.1 (sm_100a)"; }
 uint64_t hj_kernel_launch_count(void) { return hj::launch_count(); }
 
@@ -597,24 +623,28 @@ hj_status hj_sort_by_workload(hj_index* ix, void* stream, uint64_t* total_candid
     cudaStream_t st = as_stream(stream);
     if (!ix->have_workload) {
         uint32_t nC = ix->nC;
+        // a previous attempt that failed part-way may have left these allocated
+        dfree(ix->cell_nb, st);
+        dfree(ix->cell_order, st);
+        Scratch tmp(st);
         unsigned long long* work = nullptr;
         uint32_t *keys = nullptr, *keys_tmp = nullptr, *vals_tmp = nullptr, *dmax = nullptr;
         uint64_t* dsum = nullptr;
         HJ_TRY(dalloc(&ix->cell_nb, nC, st));
-        HJ_TRY(dalloc(&work, nC, st));
+        HJ_TRY(tmp.alloc(&work, nC));
         unsigned g = (unsigned)(((uint64_t)nC * 32 + 255) / 256);
         k_cell_workload<<<g, 256, 0, st>>>(ix->cell_lid, ix->cell_start, nC, ix->grid, cell_hash(ix), ix->cell_nb,
                                            work);
         HJ_LAUNCHED();
-        HJ_TRY(dalloc(&dsum, 1, st));
+        HJ_TRY(tmp.alloc(&dsum, 1));
         HJ_TRY(reduce_sum_u64(reinterpret_cast<uint64_t*>(work), nC, dsum, st));
-        HJ_TRY(dalloc(&dmax, 1, st));
+        HJ_TRY(tmp.alloc(&dmax, 1));
         HJ_CUDA(cudaMemsetAsync(dmax, 0, 4, st));
         k_max_u32<<<std::min<unsigned>((nC + 255) / 256, num_sms() * 4), 256, 0, st>>>(ix->cell_nb, nC, dmax);
         HJ_LAUNCHED();
-        HJ_TRY(dalloc(&keys, nC, st));
-        HJ_TRY(dalloc(&keys_tmp, nC, st));
-        HJ_TRY(dalloc(&vals_tmp, nC, st));
+        HJ_TRY(tmp.alloc(&keys, nC));
+        HJ_TRY(tmp.alloc(&keys_tmp, nC));
+        HJ_TRY(tmp.alloc(&vals_tmp, nC));
         HJ_TRY(dalloc(&ix->cell_order, nC, st));
         k_desc_keys<<<(nC + 255) / 256, 256, 0, st>>>(ix->cell_nb, nC, keys, ix->cell_order);
         HJ_LAUNCHED();
@@ -624,12 +654,6 @@ hj_status hj_sort_by_workload(hj_index* ix, void* stream, uint64_t* total_candid
         HJ_CUDA(cudaMemcpyAsync(&ix->max_nb, dmax, 4, cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
         ix->total_candidates = tot;
-        dfree(work, st);
-        dfree(keys, st);
-        dfree(keys_tmp, st);
-        dfree(vals_tmp, st);
-        dfree(dmax, st);
-        dfree(dsum, st);
         ix->have_workload = true;
     }
     if (total_candidates) *total_candidates = ix->total_candidates;
@@ -645,15 +669,15 @@ hj_status hj_workload_export(const hj_index* ix, hj_scheduling_cell* d_sched, ui
         HJ_LAUNCHED();
     }
     if (d_origin) {
+        Scratch tmp(st);
         uint32_t* off = nullptr;
-        HJ_TRY(dalloc(&off, nC, st));
+        HJ_TRY(tmp.alloc(&off, nC));
         k_pop_in_order<<<(nC + 255) / 256, 256, 0, st>>>(ix->cell_order, ix->cell_start, nC, off);
         HJ_LAUNCHED();
         HJ_TRY(scan_u32_inplace(off, nC, st));
         k_origin_index<<<(unsigned)(((uint64_t)nC * 32 + 255) / 256), 256, 0, st>>>(ix->cell_order, ix->cell_start,
                                                                                    ix->perm, off, nC, d_origin);
         HJ_LAUNCHED();
-        dfree(off, st);
     }
     return HJ_OK;
 }

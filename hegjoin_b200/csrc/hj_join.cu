@@ -28,6 +28,7 @@
 #include <fstream>
 #include <map>
 #include <mutex>
+#include <queue>
 #include <sstream>
 
 #include "hj_internal.h"
@@ -45,7 +46,9 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
                            cudaStream_t st);
 hj_status launch_band_recheck(const hj_index* ix, const uint32_t* bq, const uint32_t* bc,
                               const unsigned long long* band_used, unsigned long long band_cap,
-                              const PairSink& sink, cudaStream_t st);
+                              const PairSink& sink, uint32_t nblocks, cudaStream_t st);
+uint64_t plain_emit_warps(uint32_t nblocks);
+uint64_t tc_emit_warps(uint32_t nblocks);
 double tc_delta(const hj_index* ix);
 double tc_band_ratio(const hj_index* ix);
 bool tc_supported(const hj_index* ix, int kind);
@@ -73,12 +76,6 @@ __global__ void k_pick_samples(const HjBlock* __restrict__ blocks, uint32_t nblo
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nsamp) return;
     out[i] = blocks[min(nblocks - 1, i * stride)];
-}
-
-__global__ void k_pick_strided(const HjBlock* __restrict__ blocks, uint32_t first, uint32_t stride, uint32_t m,
-                               HjBlock* __restrict__ out) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) out[i] = blocks[first + i * stride];
 }
 
 // Number of non-sentinel keys in a sorted key array (sentinels sort last).
@@ -240,58 +237,114 @@ namespace hj {
 void result_set_stream(hj_result* r, cudaStream_t s) {
     if (r) r->stream = s;
 }
-}  // namespace hj
 
-using namespace hj;
+namespace {
 
-extern "C" {
+__global__ void k_pick_list(const HjBlock* __restrict__ blocks, const uint32_t* __restrict__ items, uint32_t m,
+                            HjBlock* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = blocks[items[i]];
+}
 
-hj_status hj_shard_plan(uint32_t n_items, uint32_t shard_count, uint32_t shard_index, uint32_t* first,
-                        uint32_t* stride, uint32_t* n_mine) {
-    if (shard_count == 0 || shard_index >= shard_count || !first || !stride || !n_mine) {
-        set_error("hj_shard_plan: shard_index %u out of range for %u shards", shard_index, shard_count);
-        return HJ_ERR_INVALID;
+// Per-query digest of one grouped batch, added into (count, sum, xor): warps
+// take 32 consecutive pairs, reduce each run of equal query ids with a
+// segmented scan, and the last lane of a run adds it with three atomics.
+__global__ void k_digest_accumulate(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                    unsigned long long n, uint32_t* __restrict__ cnt,
+                                    unsigned long long* __restrict__ sum, unsigned long long* __restrict__ xr) {
+    const uint32_t lane = lane_id();
+    const unsigned long long warps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+    for (unsigned long long base = (((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32ull;
+         base < n; base += warps * 32ull) {
+        const unsigned long long i = base + lane;
+        const bool valid = i < n;
+        const uint32_t key = valid ? keys[i] : kSentinelKey;
+        const uint32_t v = valid ? vals[i] : 0u;
+        unsigned long long s = valid ? mix64(v) : 0ull;
+        unsigned long long x = valid ? mix64((uint64_t)v ^ 0x5bd1e9955bd1e995ull) : 0ull;
+        uint32_t c = valid ? 1u : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t k2 = __shfl_up_sync(0xffffffffu, key, o);
+            const unsigned long long s2 = __shfl_up_sync(0xffffffffu, s, o);
+            const unsigned long long x2 = __shfl_up_sync(0xffffffffu, x, o);
+            const uint32_t c2 = __shfl_up_sync(0xffffffffu, c, o);
+            if (lane >= (uint32_t)o && k2 == key) {   // keys are sorted: equal keys are contiguous
+                s += s2;
+                x ^= x2;
+                c += c2;
+            }
+        }
+        const uint32_t next = __shfl_down_sync(0xffffffffu, key, 1);
+        if (valid && (lane == 31 || next != key)) {
+            atomicAdd(&cnt[key], c);
+            atomicAdd(&sum[key], s);
+            atomicXor(&xr[key], x);
+        }
     }
-    // round robin over the heaviest-first order: every rank gets a mix of heavy
-    // and light items (an LPT-like balance without a host pass over item costs)
-    *first = shard_index;
-    *stride = shard_count;
-    *n_mine = n_items > shard_index ? (n_items - shard_index + shard_count - 1) / shard_count : 0;
-    return HJ_OK;
 }
 
-void hj_join_opts_default(hj_join_opts* o) {
-    if (!o) return;
-    *o = hj_join_opts{};
-    o->refine = HJ_REFINE_AUTO;
-    o->sample_rate = 0.02;
-    o->mem_fraction = 0.6;
-    o->use_graphs = 0;
-    o->keep_keys = 0;
+// Timing events are taken from a per-thread pool and returned to it: creating and
+// destroying them per launch is a driver call each, which concurrent joins (the
+// serving loop's workers) would serialise on.
+struct EventPool {
+    std::vector<cudaEvent_t> free;
+    ~EventPool() {
+        for (cudaEvent_t e : free) cudaEventDestroy(e);
+    }
+};
+thread_local EventPool t_events;
+
+hj_status event_acquire(cudaEvent_t* e) {
+    if (!t_events.free.empty()) {
+        *e = t_events.free.back();
+        t_events.free.pop_back();
+        return HJ_OK;
+    }
+    return cuda_status(cudaEventCreate(e), "cudaEventCreate");
 }
 
-hj_status hj_result_destroy(hj_result* r) {
-    if (!r) return HJ_OK;
-    for (auto* p : r->vals) cudaFreeAsync(p, r->stream);
-    for (auto* p : r->keys) cudaFreeAsync(p, r->stream);
-    if (r->d_batch_vals) cudaFreeAsync(r->d_batch_vals, r->stream);
-    if (r->table) cudaFreeAsync(r->table, r->stream);
-    delete r;
-    return HJ_OK;
-}
+// CUDA events of the refine launches, returned to the pool on every return path.
+struct EventPairs {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    ~EventPairs() {
+        for (auto& e : ev) {
+            if (e.first) t_events.free.push_back(e.first);
+            if (e.second) t_events.free.push_back(e.second);
+        }
+    }
+};
 
-hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_result** out, hj_join_stats* stats) {
+// What a join does with each grouped batch.
+struct BatchHandler {
+    virtual ~BatchHandler() = default;
+    // `count` pairs of batch `batch`: query ids (ascending) in keys, neighbour ids
+    // grouped by query in vals.  Both live in the join's reusable buffers and stay
+    // valid in the order of `st` until the next batch's refine is enqueued.
+    virtual hj_status on_batch(uint32_t batch, const uint32_t* keys, const uint32_t* vals, uint64_t count,
+                               cudaStream_t st) = 0;
+};
+
+// The batched join (distanceTableNDGridBatches, GPU.cu:787-1702): refine kind,
+// work items (optionally this rank's share), estimator, result-buffer sizing,
+// batches with overflow split-and-retry, grouping by query id.  Every device
+// temporary lives in `tmp` and is freed on every return path.
+// kept_bytes_per_pair: device bytes the handler keeps per result pair (left free).
+hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, BatchHandler& handler,
+                    double kept_bytes_per_pair, hj_join_stats* stats) {
     auto t_start = std::chrono::steady_clock::now();
-    if (!ix || !out) { set_error("hj_join: null argument"); return HJ_ERR_INVALID; }
-    *out = nullptr;
     hj_join_opts opts;
     if (opts_in) opts = *opts_in; else hj_join_opts_default(&opts);
     if (opts.sample_rate <= 0 || opts.sample_rate > 1) opts.sample_rate = 0.02;
     if (opts.mem_fraction <= 0 || opts.mem_fraction > 0.95) opts.mem_fraction = 0.6;
-    cudaStream_t st = as_stream(stream);
+    if (opts.shard_count > 1 && opts.shard_index >= opts.shard_count) {
+        set_error("hj_join: shard_index %u out of range for %u shards", opts.shard_index, opts.shard_count);
+        return HJ_ERR_INVALID;
+    }
+    Scratch tmp(st);
     uint64_t launches0 = thread_launch_count();
     hj_join_stats S{};
-    HJ_TRY(hj_sort_by_workload(ix, stream, nullptr));
+    HJ_TRY(hj_sort_by_workload(ix, st, nullptr));
 
     // ---- refine kind
     int refine = opts.refine;
@@ -316,58 +369,74 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         if (tc) S.filter_delta = tc_delta(ix);
     }
     S.refine_used = (uint32_t)refine;
-    uint32_t qb = opts.query_block ? opts.query_block : (tc ? tc_query_block() : plain_query_block(ix->dtype));
-    if (tc) qb = tc_query_block();   // the tensor-core tile shape fixes the block size
-    if (!tc && qb != plain_query_block(ix->dtype)) qb = plain_query_block(ix->dtype);
+    // the tile shape of each refine kernel fixes its work-item size
+    const uint32_t qb = tc ? tc_query_block() : plain_query_block(ix->dtype);
 
     HjBlock* blocks = nullptr;
     uint32_t nblocks = 0;
     HJ_TRY(build_blocks(ix, qb, &blocks, &nblocks, st));
+    tmp.adopt(blocks);
+    std::vector<HjBlock> hblocks(nblocks);
+    if (nblocks) {
+        HJ_CUDA(cudaMemcpyAsync(hblocks.data(), blocks, (size_t)nblocks * sizeof(HjBlock), cudaMemcpyDeviceToHost, st));
+        HJ_CUDA(cudaStreamSynchronize(st));
+    }
     if (opts.shard_count > 1) {
-        // this rank's share of the heaviest-first order
-        uint32_t first = 0, stride = 1, mine = 0;
-        HJ_TRY(hj_shard_plan(nblocks, opts.shard_count, opts.shard_index, &first, &stride, &mine));
+        // this rank's share of the items: greedy LPT on (candidates x queries) per item
+        std::vector<uint64_t> cost(nblocks);
+        for (uint32_t i = 0; i < nblocks; ++i) cost[i] = (uint64_t)hblocks[i].nb * (hblocks[i].q1 - hblocks[i].q0);
+        std::vector<uint32_t> mine(std::max<uint32_t>(nblocks, 1));
+        uint32_t n_mine = 0;
+        HJ_TRY(hj_shard_plan_lpt(cost.data(), nblocks, opts.shard_count, opts.shard_index, mine.data(), &n_mine));
+        uint32_t* d_items = nullptr;
         HjBlock* sel = nullptr;
-        HJ_TRY(dalloc(&sel, std::max<uint32_t>(mine, 1), st));
-        if (mine) {
-            k_pick_strided<<<(mine + 255) / 256, 256, 0, st>>>(blocks, first, stride, mine, sel);
+        HJ_TRY(tmp.alloc(&d_items, std::max<uint32_t>(n_mine, 1)));
+        HJ_TRY(tmp.alloc(&sel, std::max<uint32_t>(n_mine, 1)));
+        if (n_mine) {
+            HJ_CUDA(cudaMemcpyAsync(d_items, mine.data(), (size_t)n_mine * 4, cudaMemcpyHostToDevice, st));
+            k_pick_list<<<(n_mine + 255) / 256, 256, 0, st>>>(blocks, d_items, n_mine, sel);
             HJ_LAUNCHED();
         }
-        dfree(blocks, st);
+        std::vector<HjBlock> hsel(n_mine);
+        for (uint32_t i = 0; i < n_mine; ++i) hsel[i] = hblocks[mine[i]];
+        hblocks.swap(hsel);
+        HJ_CUDA(cudaStreamSynchronize(st));   // the host copy of the item list is read by the copy above
+        tmp.release(blocks);
+        tmp.release(d_items);
         blocks = sel;
-        nblocks = mine;
+        nblocks = n_mine;
     }
 
     unsigned int* head = nullptr;
     // [0] pair cursor, [1] valid count, [2] tc accepts, [3] tc band pairs, [4] band cursor
     unsigned long long* counters = nullptr;
     uint32_t* flags = nullptr;                 // [0] overflow, [1] bounded-wait timeout
-    HJ_TRY(dalloc(&head, 1, st));
-    HJ_TRY(dalloc(&counters, 8, st));
-    HJ_TRY(dalloc(&flags, 2, st));
+    HJ_TRY(tmp.alloc(&head, 1));
+    HJ_TRY(tmp.alloc(&counters, 8));
+    HJ_TRY(tmp.alloc(&flags, 2));
     HJ_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
     HJ_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), st));
     uint32_t* overflow = flags;
     PairSink no_band{nullptr, nullptr, nullptr, 0, overflow};
 
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kev;   // refine kernel launches of the join proper
+    EventPairs kev;   // refine kernel launches of the join proper
     auto run_refine = [&](const HjBlock* blk, uint32_t nb, const PairSink& sink, const PairSink& band,
                           uint32_t count_only, unsigned long long* bc) -> hj_status {
         HJ_CUDA(cudaMemsetAsync(head, 0, sizeof(unsigned int), st));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (!count_only) {
-            HJ_CUDA(cudaEventCreate(&e0));
-            HJ_CUDA(cudaEventCreate(&e1));
+            kev.ev.emplace_back(nullptr, nullptr);
+            HJ_TRY(event_acquire(&kev.ev.back().first));
+            HJ_TRY(event_acquire(&kev.ev.back().second));
+            e0 = kev.ev.back().first;
+            e1 = kev.ev.back().second;
             HJ_CUDA(cudaEventRecord(e0, st));
         }
-        hj_status r = tc ? launch_refine_tc(ix, blk, nb, head, sink, band, count_only, bc,
-                                            count_only ? nullptr : counters + 2, flags + 1, st)
-                         : launch_refine_plain(ix, blk, nb, head, sink, count_only, bc, st);
-        if (!count_only) {
-            HJ_CUDA(cudaEventRecord(e1, st));
-            kev.emplace_back(e0, e1);
-        }
-        return r;
+        HJ_TRY(tc ? launch_refine_tc(ix, blk, nb, head, sink, band, count_only, bc,
+                                     count_only ? nullptr : counters + 2, flags + 1, st)
+                  : launch_refine_plain(ix, blk, nb, head, sink, count_only, bc, st));
+        if (!count_only) HJ_CUDA(cudaEventRecord(e1, st));
+        return HJ_OK;
     };
     auto check_timeout = [&]() -> hj_status {
         uint32_t to = 0;
@@ -382,8 +451,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
 
     // ---- estimator (GPUBatchEst_v2, GPU.cu:403-779)
     auto t_est = std::chrono::steady_clock::now();
-    std::vector<HjBlock> hblocks(nblocks);
-    if (nblocks) HJ_CUDA(cudaMemcpyAsync(hblocks.data(), blocks, (size_t)nblocks * sizeof(HjBlock), cudaMemcpyDeviceToHost, st));
+    S.ms_setup = ms_since(t_start);
     uint32_t stride = std::max<uint32_t>(1, (uint32_t)std::lround(1.0 / opts.sample_rate));
     uint32_t nsamp = nblocks ? (nblocks + stride - 1) / stride : 0;
     std::vector<double> est(nblocks, 0.0);
@@ -391,8 +459,8 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     if (nsamp) {
         HjBlock* sblocks = nullptr;
         unsigned long long* scnt = nullptr;
-        HJ_TRY(dalloc(&sblocks, nsamp, st));
-        HJ_TRY(dalloc(&scnt, nsamp, st));
+        HJ_TRY(tmp.alloc(&sblocks, nsamp));
+        HJ_TRY(tmp.alloc(&scnt, nsamp));
         HJ_CUDA(cudaMemsetAsync(scnt, 0, nsamp * sizeof(unsigned long long), st));
         k_pick_samples<<<(nsamp + 255) / 256, 256, 0, st>>>(blocks, nblocks, stride, nsamp, sblocks);
         HJ_LAUNCHED();
@@ -408,7 +476,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
                 std::vector<unsigned long long> h0(nsamp);
                 HJ_CUDA(cudaMemcpyAsync(h0.data(), scnt, nsamp * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                         st));
-                HJ_CUDA(cudaStreamSynchronize(st));   // also completes the copy of hblocks
+                HJ_CUDA(cudaStreamSynchronize(st));
                 double sp = 0, sc = 0;
                 for (uint32_t q = 0; q < nsamp; ++q) {
                     const HjBlock& b = hblocks[std::min(nblocks - 1, q * stride)];
@@ -422,22 +490,21 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
             const int cands[4] = {2, 4, 10, 12};
             float best = 1e30f;
             int best_epi = tc_get_epi(ix);
-            cudaEvent_t e0, e1;
-            HJ_CUDA(cudaEventCreate(&e0));
-            HJ_CUDA(cudaEventCreate(&e1));
+            EventPairs tev;
+            tev.ev.emplace_back(nullptr, nullptr);
+            HJ_TRY(event_acquire(&tev.ev[0].first));
+            HJ_TRY(event_acquire(&tev.ev[0].second));
             for (int c : cands) {
                 tc_set_epi(ix, c);
                 HJ_CUDA(cudaMemsetAsync(scnt, 0, nsamp * sizeof(unsigned long long), st));
-                HJ_CUDA(cudaEventRecord(e0, st));
+                HJ_CUDA(cudaEventRecord(tev.ev[0].first, st));
                 HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
-                HJ_CUDA(cudaEventRecord(e1, st));
+                HJ_CUDA(cudaEventRecord(tev.ev[0].second, st));
                 HJ_TRY(check_timeout());
                 float ms = 0;
-                HJ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                HJ_CUDA(cudaEventElapsedTime(&ms, tev.ev[0].first, tev.ev[0].second));
                 if (ms < best) { best = ms; best_epi = c; }
             }
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
             tc_set_epi(ix, best_epi);
             tune_store(key, best_epi);
         } else {
@@ -448,8 +515,8 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         std::vector<unsigned long long> hs(nsamp);
         HJ_CUDA(cudaMemcpyAsync(hs.data(), scnt, nsamp * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
-        dfree(sblocks, st);
-        dfree(scnt, st);
+        tmp.release(sblocks);
+        tmp.release(scnt);
         std::vector<double> rate(nsamp);
         for (uint32_t s = 0; s < nsamp; ++s) {
             const HjBlock& b = hblocks[std::min(nblocks - 1, s * stride)];
@@ -461,8 +528,6 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
             est[i] = r * (hblocks[i].q1 - hblocks[i].q0);
             total_est += est[i];
         }
-    } else {
-        HJ_CUDA(cudaStreamSynchronize(st));
     }
     S.estimated_pairs = (uint64_t)total_est;
     S.ms_estimate = ms_since(t_est);
@@ -473,18 +538,30 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     }
 
     // ---- result buffer capacity
-    size_t free_b = 0, total_b = 0;
-    HJ_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const uint64_t chunk_slack = (uint64_t)num_sms() * 64 * kSinkChunk;   // partially filled warp chunks
-    const double bytes_per_slot = 16.0 + 4.0 + (opts.keep_keys ? 4.0 : 0.0) + (tc ? 8.0 : 0.0);
-    // leave room for the result itself (4 bytes per estimated pair, kept on the device)
-    const double result_bytes = 4.0 * total_est * (opts.keep_keys ? 2.0 : 1.0) * 1.1;
-    const double usable = std::max(0.0, (double)free_b - result_bytes);
-    uint64_t max_cap = (uint64_t)(opts.mem_fraction * usable / bytes_per_slot);
-    max_cap = std::min<uint64_t>(max_cap, 0xF0000000ull);
-    uint64_t want = (uint64_t)(total_est * 2.0) + chunk_slack + 4096;
-    uint64_t cap = opts.result_capacity ? opts.result_capacity + chunk_slack : std::min(want, max_cap);
-    if (cap < chunk_slack * 2) cap = std::min<uint64_t>(chunk_slack * 2, max_cap);
+    // slack for partly filled warp chunks: every warp that can emit during a batch holds
+    // at most one (sized from the launch grids, so small joins get small buffers)
+    const uint64_t chunk_slack = (tc ? tc_emit_warps(nblocks) : plain_emit_warps(nblocks)) * kSinkChunk;
+    const uint32_t slot_words = tc ? 6u : 4u;   // keys, vals, their radix copies (+ band pair ids)
+    const double bytes_per_slot = 4.0 * slot_words;
+    const uint64_t want = (uint64_t)(total_est * 2.0) + chunk_slack + 4096;
+    uint64_t cap = opts.result_capacity ? opts.result_capacity + chunk_slack : want;
+    if (cap < chunk_slack * 2) cap = chunk_slack * 2;
+    // the device-wide free-memory query (a driver call) only when the buffers are large
+    const double result_bytes = kept_bytes_per_pair * total_est * 1.1;   // what the handler keeps
+    auto max_cap_from_free = [&](uint64_t* out) -> hj_status {
+        size_t free_b = 0, total_b = 0;
+        HJ_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const double usable = std::max(0.0, (double)free_b - result_bytes);
+        *out = std::min<uint64_t>((uint64_t)(opts.mem_fraction * usable / bytes_per_slot), 0xF0000000ull);
+        return HJ_OK;
+    };
+    const bool large = (double)cap * bytes_per_slot + result_bytes > 1024.0 * 1024 * 1024;
+    if (large) {
+        uint64_t max_cap = 0;
+        HJ_TRY(max_cap_from_free(&max_cap));
+        cap = std::min(cap, max_cap);
+    }
+    cap = std::min<uint64_t>(cap, 0xF0000000ull);   // radix sort and 32-bit counts per batch
     if (cap <= chunk_slack) {
         set_error("hj_join: not enough device memory for a result buffer");
         return HJ_ERR_OOM;
@@ -508,48 +585,44 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
     }
     std::reverse(batches.begin(), batches.end());   // used as a stack
 
-    uint32_t *keys = nullptr, *vals = nullptr, *keys_tmp = nullptr, *vals_tmp = nullptr;
-    uint32_t *band_q = nullptr, *band_c = nullptr;
-    HJ_TRY(dalloc(&keys, cap, st));
-    HJ_TRY(dalloc(&vals, cap, st));
-    HJ_TRY(dalloc(&keys_tmp, cap, st));
-    HJ_TRY(dalloc(&vals_tmp, cap, st));
-    if (tc) {
-        HJ_TRY(dalloc(&band_q, cap, st));
-        HJ_TRY(dalloc(&band_c, cap, st));
+    // one allocation carved into keys, vals, their radix copies and the band pair ids;
+    // when the free-memory query was skipped and the allocation fails, query and retry smaller
+    uint32_t* slab = nullptr;
+    hj_status as = tmp.alloc(&slab, cap * slot_words);
+    if (as == HJ_ERR_OOM && !large && !opts.result_capacity) {
+        uint64_t max_cap = 0;
+        HJ_TRY(max_cap_from_free(&max_cap));
+        if (max_cap < cap && max_cap > chunk_slack) {
+            cap = max_cap;
+            as = tmp.alloc(&slab, cap * slot_words);
+        }
     }
-
-    hj_result* res = new hj_result();
-    res->n = ix->n;
-    res->stream = st;
-    hj_status rs = dalloc(&res->table, ix->n, st);
-    if (rs != HJ_OK) { delete res; return rs; }
-    HJ_CUDA(cudaMemsetAsync(res->table, 0, (size_t)ix->n * sizeof(hj_nt_entry), st));
+    HJ_TRY(as);
+    uint32_t *keys = slab, *vals = slab + cap, *keys_tmp = slab + 2 * cap, *vals_tmp = slab + 3 * cap;
+    uint32_t* band_q = tc ? slab + 4 * cap : nullptr;
+    uint32_t* band_c = tc ? slab + 5 * cap : nullptr;
     const uint32_t key_bits = bits_for(ix->n);
 
     auto t_ref = std::chrono::steady_clock::now();
     float ms_group = 0;
-    hj_status status = HJ_OK;
+    uint64_t total = 0;
+    uint32_t n_out = 0;
     while (!batches.empty()) {
         Batch b = batches.back();
         batches.pop_back();
-        if (opts.max_batches && res->vals.size() >= opts.max_batches) {
+        if (opts.max_batches && n_out >= opts.max_batches) {
             set_error("hj_join: batch limit %u reached", opts.max_batches);
-            status = HJ_ERR_OVERFLOW;
-            break;
+            return HJ_ERR_OVERFLOW;
         }
         HJ_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st));
         HJ_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), st));
         HJ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(uint32_t), st));
         PairSink sink{keys, vals, counters, cap, overflow};
         PairSink band = tc ? PairSink{band_q, band_c, counters + 4, cap, overflow} : no_band;
-        status = run_refine(blocks + b.b0, b.b1 - b.b0, sink, band, 0, nullptr);
-        if (status != HJ_OK) break;
+        HJ_TRY(run_refine(blocks + b.b0, b.b1 - b.b0, sink, band, 0, nullptr));
         if (tc) {
-            status = launch_band_recheck(ix, band_q, band_c, counters + 4, cap, sink, st);
-            if (status != HJ_OK) break;
-            status = check_timeout();
-            if (status != HJ_OK) break;
+            HJ_TRY(launch_band_recheck(ix, band_q, band_c, counters + 4, cap, sink, b.b1 - b.b0, st));
+            HJ_TRY(check_timeout());
         }
         unsigned long long used = 0;
         uint32_t ovf = 0;
@@ -560,8 +633,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
             if (b.b1 - b.b0 <= 1) {
                 set_error("hj_join: one work item produces more pairs than the result buffer holds (%llu)",
                           (unsigned long long)cap);
-                status = HJ_ERR_OVERFLOW;
-                break;
+                return HJ_ERR_OVERFLOW;
             }
             uint32_t mid = b.b0 + (b.b1 - b.b0) / 2;
             batches.push_back({mid, b.b1});
@@ -571,8 +643,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         }
         auto t_g = std::chrono::steady_clock::now();
         uint64_t slots = std::min<uint64_t>(used, cap);
-        status = radix_sort_u32_u32(keys, vals, keys_tmp, vals_tmp, slots, key_bits, st);
-        if (status != HJ_OK) break;
+        HJ_TRY(radix_sort_u32_u32(keys, vals, keys_tmp, vals_tmp, slots, key_bits, st));
         unsigned long long valid = 0;
         if (slots) {
             k_count_valid<<<(unsigned)((slots + 255) / 256), 256, 0, st>>>(keys, slots, counters + 1);
@@ -580,35 +651,17 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
             HJ_CUDA(cudaMemcpyAsync(&valid, counters + 1, 8, cudaMemcpyDeviceToHost, st));
             HJ_CUDA(cudaStreamSynchronize(st));
         }
-        uint32_t bi = (uint32_t)res->vals.size();
-        uint32_t* bv = nullptr;
-        status = dalloc(&bv, valid, st);
-        if (status != HJ_OK) break;
-        if (valid) HJ_CUDA(cudaMemcpyAsync(bv, vals, valid * 4, cudaMemcpyDeviceToDevice, st));
-        res->vals.push_back(bv);
-        res->counts.push_back(valid);
-        if (opts.keep_keys) {
-            uint32_t* bk = nullptr;
-            status = dalloc(&bk, valid, st);
-            if (status != HJ_OK) break;
-            if (valid) HJ_CUDA(cudaMemcpyAsync(bk, keys, valid * 4, cudaMemcpyDeviceToDevice, st));
-            res->keys.push_back(bk);
-        }
-        if (valid) {
-            k_table<<<(unsigned)((valid + 255) / 256), 256, 0, st>>>(keys, valid, bi, res->table);
-            HJ_LAUNCHED();
-        }
-        res->total += valid;
+        HJ_TRY(handler.on_batch(n_out, keys, vals, valid, st));
+        ++n_out;
+        total += valid;
         ms_group += ms_since(t_g);
     }
     HJ_CUDA(cudaStreamSynchronize(st));
     S.ms_refine = ms_since(t_ref) - ms_group;
     S.ms_group = ms_group;
-    for (auto& ev : kev) {
+    for (auto& ev : kev.ev) {
         float ms = 0;
         if (cudaEventElapsedTime(&ms, ev.first, ev.second) == cudaSuccess) S.ms_refine_kernel += ms;
-        cudaEventDestroy(ev.first);
-        cudaEventDestroy(ev.second);
         S.refine_launches++;
     }
     cudaGetLastError();
@@ -619,27 +672,188 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts_in, void* stream, hj_re
         S.tc_accepts = tcs[0];
         S.band_pairs = tcs[1];
     }
-    dfree(keys, st); dfree(vals, st); dfree(keys_tmp, st); dfree(vals_tmp, st);
-    dfree(band_q, st); dfree(band_c, st);
-    dfree(blocks, st); dfree(head, st); dfree(counters, st); dfree(flags, st);
-    if (status == HJ_OK && !res->vals.empty()) {
-        hj_status s2 = dalloc(&res->d_batch_vals, res->vals.size(), st);
-        if (s2 == HJ_OK)
-            s2 = cudaMemcpyAsync(res->d_batch_vals, res->vals.data(), res->vals.size() * sizeof(uint32_t*),
-                                 cudaMemcpyHostToDevice, st) == cudaSuccess ? HJ_OK : HJ_ERR_CUDA;
-        status = s2;
-    }
-    cudaStreamSynchronize(st);
-    if (status != HJ_OK) {
-        hj_result_destroy(res);
-        return status;
-    }
-    S.total_pairs = res->total;
-    S.n_batches = (uint32_t)res->vals.size();
+    S.total_pairs = total;
+    S.n_batches = n_out;
     S.ms_total = ms_since(t_start);
     S.kernel_launches = (uint32_t)(thread_launch_count() - launches0);
     if (stats) *stats = S;
+    return HJ_OK;
+}
+
+// hj_join: every batch's neighbour ids stay on the device (a copy per batch) and
+// the device neighbour table points into them.
+struct RetainHandler : BatchHandler {
+    hj_result* res;
+    bool keep_keys;
+    RetainHandler(hj_result* r, bool kk) : res(r), keep_keys(kk) {}
+    hj_status on_batch(uint32_t bi, const uint32_t* keys, const uint32_t* vals, uint64_t count,
+                       cudaStream_t st) override {
+        uint32_t* bv = nullptr;
+        HJ_TRY(dalloc(&bv, count, st));
+        res->vals.push_back(bv);
+        res->counts.push_back(count);
+        if (count) HJ_CUDA(cudaMemcpyAsync(bv, vals, count * 4, cudaMemcpyDeviceToDevice, st));
+        if (keep_keys) {
+            uint32_t* bk = nullptr;
+            HJ_TRY(dalloc(&bk, count, st));
+            res->keys.push_back(bk);
+            if (count) HJ_CUDA(cudaMemcpyAsync(bk, keys, count * 4, cudaMemcpyDeviceToDevice, st));
+        }
+        if (count) {
+            k_table<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(keys, count, bi, res->table);
+            HJ_LAUNCHED();
+        }
+        res->total += count;
+        return HJ_OK;
+    }
+};
+
+// hj_join_stream: per-query digests accumulated on the device, then the caller's
+// sink; nothing is kept after the sink returns.
+struct StreamHandler : BatchHandler {
+    hj_batch_sink sink;
+    void* user;
+    uint32_t* cnt;
+    unsigned long long* sum;
+    unsigned long long* xr;
+    StreamHandler(hj_batch_sink s, void* u, uint32_t* c, uint64_t* sm, uint64_t* x)
+        : sink(s), user(u), cnt(c), sum(reinterpret_cast<unsigned long long*>(sm)),
+          xr(reinterpret_cast<unsigned long long*>(x)) {}
+    hj_status on_batch(uint32_t bi, const uint32_t* keys, const uint32_t* vals, uint64_t count,
+                       cudaStream_t st) override {
+        if (count && cnt) {
+            const unsigned g = (unsigned)std::min<uint64_t>((count + 255) / 256, (uint64_t)num_sms() * 16);
+            k_digest_accumulate<<<g, 256, 0, st>>>(keys, vals, count, cnt, sum, xr);
+            HJ_LAUNCHED();
+        }
+        if (!sink) return HJ_OK;
+        hj_batch_view v{bi, 0u, count, keys, vals};
+        hj_status s = sink(&v, user, st);
+        if (s != HJ_OK) {
+            set_error("hj_join_stream: the batch sink returned %d", s);
+            return s;
+        }
+        return HJ_OK;
+    }
+};
+
+}  // namespace
+}  // namespace hj
+
+using namespace hj;
+
+extern "C" {
+
+hj_status hj_shard_plan(uint32_t n_items, uint32_t shard_count, uint32_t shard_index, uint32_t* first,
+                        uint32_t* stride, uint32_t* n_mine) {
+    if (shard_count == 0 || shard_index >= shard_count || !first || !stride || !n_mine) {
+        set_error("hj_shard_plan: shard_index %u out of range for %u shards", shard_index, shard_count);
+        return HJ_ERR_INVALID;
+    }
+    // round robin over the heaviest-first order
+    *first = shard_index;
+    *stride = shard_count;
+    *n_mine = n_items > shard_index ? (n_items - shard_index + shard_count - 1) / shard_count : 0;
+    return HJ_OK;
+}
+
+hj_status hj_shard_plan_lpt(const uint64_t* costs, uint32_t n_items, uint32_t shard_count, uint32_t shard_index,
+                            uint32_t* items, uint32_t* n_mine) {
+    if (shard_count == 0 || shard_index >= shard_count || !n_mine || (n_items && (!costs || !items))) {
+        set_error("hj_shard_plan_lpt: invalid arguments (%u items, shard %u of %u)", n_items, shard_index,
+                  shard_count);
+        return HJ_ERR_INVALID;
+    }
+    // longest processing time first: items by cost, descending (ties by index), each to
+    // the least-loaded shard (ties to the lowest shard index); every rank computes the
+    // same assignment from the same costs
+    std::vector<uint32_t> order(n_items);
+    for (uint32_t i = 0; i < n_items; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return costs[a] > costs[b]; });
+    using Load = std::pair<uint64_t, uint32_t>;   // (load, shard)
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (uint32_t s = 0; s < shard_count; ++s) heap.push({0, s});
+    std::vector<uint8_t> mine(n_items, 0);
+    for (uint32_t i : order) {
+        Load l = heap.top();
+        heap.pop();
+        if (l.second == shard_index) mine[i] = 1;
+        l.first += costs[i];
+        heap.push(l);
+    }
+    uint32_t m = 0;
+    for (uint32_t i = 0; i < n_items; ++i)
+        if (mine[i]) items[m++] = i;   // ascending: the heaviest-first order within the shard
+    *n_mine = m;
+    return HJ_OK;
+}
+
+void hj_join_opts_default(hj_join_opts* o) {
+    if (!o) return;
+    *o = hj_join_opts{};
+    o->refine = HJ_REFINE_AUTO;
+    o->sample_rate = 0.02;
+    o->mem_fraction = 0.6;
+    o->use_graphs = 0;
+    o->keep_keys = 0;
+}
+
+hj_status hj_result_destroy(hj_result* r) {
+    if (!r) return HJ_OK;
+    for (auto* p : r->vals) cudaFreeAsync(p, r->stream);
+    for (auto* p : r->keys) cudaFreeAsync(p, r->stream);
+    if (r->d_batch_vals) cudaFreeAsync(r->d_batch_vals, r->stream);
+    if (r->table) cudaFreeAsync(r->table, r->stream);
+    delete r;
+    return HJ_OK;
+}
+
+hj_status hj_join(hj_index* ix, const hj_join_opts* opts, void* stream, hj_result** out, hj_join_stats* stats) {
+    if (!ix || !out) { set_error("hj_join: null argument"); return HJ_ERR_INVALID; }
+    *out = nullptr;
+    cudaStream_t st = as_stream(stream);
+    hj_result* res = new hj_result();
+    res->n = ix->n;
+    res->stream = st;
+    hj_status s = dalloc(&res->table, ix->n, st);
+    if (s == HJ_OK) s = cuda_status(cudaMemsetAsync(res->table, 0, (size_t)ix->n * sizeof(hj_nt_entry), st),
+                                    "clear the neighbour table");
+    const bool keep_keys = opts && opts->keep_keys;
+    RetainHandler h(res, keep_keys);
+    hj_join_stats S{};
+    if (s == HJ_OK) s = join_impl(ix, opts, st, h, keep_keys ? 8.0 : 4.0, &S);
+    if (s == HJ_OK && !res->vals.empty()) {
+        s = dalloc(&res->d_batch_vals, res->vals.size(), st);
+        if (s == HJ_OK)
+            s = cuda_status(cudaMemcpyAsync(res->d_batch_vals, res->vals.data(), res->vals.size() * sizeof(uint32_t*),
+                                            cudaMemcpyHostToDevice, st), "batch pointer table");
+    }
+    if (s == HJ_OK) s = cuda_status(cudaStreamSynchronize(st), "hj_join");
+    if (s != HJ_OK) {
+        hj_result_destroy(res);
+        return s;
+    }
+    if (stats) *stats = S;
     *out = res;
+    return HJ_OK;
+}
+
+hj_status hj_join_stream(hj_index* ix, const hj_join_opts* opts, hj_batch_sink sink, void* user, uint32_t* d_count,
+                         uint64_t* d_sum, uint64_t* d_xor, void* stream, hj_join_stats* stats) {
+    if (!ix) { set_error("hj_join_stream: null index"); return HJ_ERR_INVALID; }
+    if ((d_count != nullptr) != (d_sum != nullptr) || (d_count != nullptr) != (d_xor != nullptr)) {
+        set_error("hj_join_stream: pass all three digest arrays or none");
+        return HJ_ERR_INVALID;
+    }
+    cudaStream_t st = as_stream(stream);
+    if (d_count) {
+        HJ_CUDA(cudaMemsetAsync(d_count, 0, (size_t)ix->n * 4, st));
+        HJ_CUDA(cudaMemsetAsync(d_sum, 0, (size_t)ix->n * 8, st));
+        HJ_CUDA(cudaMemsetAsync(d_xor, 0, (size_t)ix->n * 8, st));
+    }
+    StreamHandler h(sink, user, d_count, d_sum, d_xor);
+    HJ_TRY(join_impl(ix, opts, st, h, 0.0, stats));
+    HJ_CUDA(cudaStreamSynchronize(st));
     return HJ_OK;
 }
 

@@ -20,6 +20,8 @@
 // each thread evaluates an RQ x RC register tile of (query, candidate) pairs.
 // Hits are appended with warp-aggregated reservations into the pair sink.
 
+#include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "hj_internal.h"
@@ -419,8 +421,15 @@ hj_status launch_t(const PlainArgs<T>& args, cudaStream_t st) {
     size_t smem = (size_t)(D ? D : args.d) * (QB + CB) * sizeof(T) + (QB + 2 * CB + 2 * kRowGroup + 1) * sizeof(uint32_t);
     auto kern = k_refine_plain<T, D, QB, CB, RQ, RC>;
     HJ_TRY(ensure_smem(kern, smem));
-    int per_sm = 0;
-    HJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    // resident blocks per SM, queried once per kernel and shared-memory size (a driver call)
+    static std::atomic<int> s_per_sm{0};
+    static std::atomic<size_t> s_smem{0};
+    int per_sm = s_per_sm.load(std::memory_order_relaxed);
+    if (per_sm == 0 || s_smem.load(std::memory_order_relaxed) != smem) {
+        HJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+        s_smem.store(smem, std::memory_order_relaxed);
+        s_per_sm.store(per_sm, std::memory_order_relaxed);
+    }
     if (per_sm < 1) {
         set_error("refine: %zu bytes of shared memory per block do not fit", smem);
         return HJ_ERR_UNSUPPORTED;
@@ -459,6 +468,13 @@ hj_status dispatch_t<double>(const PlainArgs<double>& a, cudaStream_t st) {
 }  // namespace
 
 uint32_t plain_query_block(int dtype) { return 64; (void)dtype; }
+
+// Upper bound on the warps of one refine launch that reserve pair-sink chunks (each
+// holds at most one partly filled chunk): at most 8 blocks of 8 warps per SM, and
+// never more blocks than work items.
+uint64_t plain_emit_warps(uint32_t nblocks) {
+    return (uint64_t)std::min<uint64_t>(8ull * num_sms(), std::max<uint32_t>(nblocks, 1)) * 8ull;
+}
 
 // Runs the exact refine over work items blocks[0..nblocks).  `head` must be
 // zero on entry.  count_only: per-item pair counts go to block_counts.

@@ -95,6 +95,7 @@ struct TcArgs {
     unsigned long long* stats;  // [0] accepted, [1] band
     uint32_t* err;
     uint32_t idesc;
+    long long wait_cycles;      // bound of every mbarrier wait (SM cycles)
 };
 
 struct TcShared {
@@ -345,7 +346,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                 TileWalk tw;
                 for (uint32_t t = 0; t < ntiles; ++t) {
                     const uint32_t s = it % a.stages, use = it / a.stages;
-                    if (use > 0 && !tc::mbar_wait(&S.empty_a[s], (use - 1) & 1u, abort, a.err, kWaitCycles)) break;
+                    if (use > 0 && !tc::mbar_wait(&S.empty_a[s], (use - 1) & 1u, abort, a.err, a.wait_cycles)) break;
                     tw.locate(S, t);
                     tc::mbar_arrive_expect_tx(&S.full_a[s], tile_bytes);
                     for (uint32_t kb = 0; kb < a.nkb; ++kb)
@@ -365,18 +366,18 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                 // and both arrive on its stage's empty barrier (count 2), so neither can run
                 // a ring cycle ahead of the other.
                 const uint32_t h = warp - 1;
-                bool ok = tc::mbar_wait(&S.bfull, items_loaded & 1u, abort, a.err, kWaitCycles);
+                bool ok = tc::mbar_wait(&S.bfull, items_loaded & 1u, abort, a.err, a.wait_cycles);
                 tc::fence_after();
                 const uint32_t ksteps = a.nkb * 2;
                 const uint32_t a_base = tc::smem_u32(a_tiles), b_base = tc::smem_u32(b_tiles);
                 const bool active = h < nqt;
                 for (uint32_t t = 0; ok && t < ntiles; ++t) {
                     const uint32_t s = it % a.stages, use = it / a.stages;
-                    if (!tc::mbar_wait(&S.full_a[s], use & 1u, abort, a.err, kWaitCycles)) break;
+                    if (!tc::mbar_wait(&S.full_a[s], use & 1u, abort, a.err, a.wait_cycles)) break;
                     tc::fence_after();
                     if (active) {
                         if (acc_use[h] > 0 &&
-                            !tc::mbar_wait(&S.empty_acc[h], (acc_use[h] - 1) & 1u, abort, a.err, kWaitCycles)) {
+                            !tc::mbar_wait(&S.empty_acc[h], (acc_use[h] - 1) & 1u, abort, a.err, a.wait_cycles)) {
                             ok = false;
                         } else {
                             tc::fence_after();
@@ -461,7 +462,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                 }
                 const uint32_t j_end = SPLIT ? min(hset + 1, nqt) : nqt;
                 for (uint32_t j = SPLIT ? hset : 0u; j < j_end; ++j) {
-                    if (!tc::mbar_wait(&S.full_acc[j], acc_use[j] & 1u, abort, a.err, kWaitCycles)) {
+                    if (!tc::mbar_wait(&S.full_acc[j], acc_use[j] & 1u, abort, a.err, a.wait_cycles)) {
                         ok = false;
                         break;
                     }
@@ -765,7 +766,8 @@ __global__ void k_fill_f32(float* p, uint32_t n, float v) {
 // sequence as k_refine_tc; writes every accumulator value to out[128][512].
 __global__ void __launch_bounds__(kProbeThreads, 1)
     k_tc_tile_probe(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query,
-                    uint32_t nkb, uint32_t idesc, uint32_t a0, uint32_t b0, float* __restrict__ out, uint32_t* err) {
+                    uint32_t nkb, uint32_t idesc, uint32_t a0, uint32_t b0, float* __restrict__ out, uint32_t* err,
+                    uint32_t skip_mma, long long wait_cycles) {
     extern __shared__ uint8_t smem_raw[];
     uint32_t base = tc::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (base & 1023u)) & 1023u);
@@ -800,9 +802,11 @@ __global__ void __launch_bounds__(kProbeThreads, 1)
         }
     }
     if (tid == 32) {
-        bool ok = tc::mbar_wait(&bars[0], 0, abortp, err, kWaitCycles);
+        // the loads always complete before this thread goes on, so with skip_mma no
+        // TMA transfer is in flight while the epilogue's wait runs out
+        bool ok = tc::mbar_wait(&bars[0], 0, abortp, err, wait_cycles);
         tc::fence_after();
-        if (ok) {
+        if (ok && !skip_mma) {
             for (uint32_t j = 0; j < kAcc; ++j)
                 for (uint32_t ks = 0; ks < nkb * 2; ++ks) {
                     const uint32_t kin = (ks & 1u) * 32u;
@@ -813,11 +817,12 @@ __global__ void __launch_bounds__(kProbeThreads, 1)
                                 idesc, ks > 0 ? 1u : 0u);
                 }
         }
-        tc::mma_commit(&bars[1]);
+        // skip_mma: no MMA and no commit, so the wait below runs out (the timeout test)
+        if (!skip_mma) tc::mma_commit(&bars[1]);
     }
     if (warp >= 2) {
         const uint32_t quarter = warp & 3u;
-        bool ok = tc::mbar_wait(&bars[1], 0, abortp, err, kWaitCycles);
+        bool ok = tc::mbar_wait(&bars[1], 0, abortp, err, wait_cycles);
         tc::fence_after();
         if (ok) {
             for (uint32_t col = 0; col < (uint32_t)kQB; col += 32) {
@@ -909,6 +914,20 @@ bool tc_supported(const hj_index* ix, int kind) {
 }
 
 uint32_t tc_query_block() { return kQB; }
+
+// Band recheck grid for a refine over nblocks work items: as many blocks as there
+// are SMs x 8, but no more than 8 per refine CTA (small joins have small bands).
+static unsigned recheck_grid(uint32_t nblocks) {
+    return (unsigned)std::min<uint64_t>((uint64_t)num_sms() * 8, 8ull * std::max<uint32_t>(1, std::min<uint32_t>(nblocks, num_sms())));
+}
+
+// Upper bound on the warps that reserve chunks of one sink during one batch: the
+// refine's epilogue warps (at most 16 per CTA, one CTA per SM) and the band
+// recheck's warps (8 per block), each holding at most one partly filled chunk.
+uint64_t tc_emit_warps(uint32_t nblocks) {
+    return (uint64_t)std::min<uint32_t>((uint32_t)num_sms(), std::max<uint32_t>(nblocks, 1)) * 16ull +
+           (uint64_t)recheck_grid(nblocks) * 8ull;
+}
 
 // Half-width of the guard band for the worst pair of the dataset, in scaled units.
 static double tc_delta_scaled(const hj_index* ix, const TcState* s) {
@@ -1106,6 +1125,7 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     a.sink = sink; a.band = band;
     a.count_only = count_only; a.block_counts = block_counts; a.stats = stats; a.err = err;
     a.idesc = tc::idesc_f16(ix->tc_kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kAccCols);
+    a.wait_cycles = kWaitCycles;
     unsigned grid = (unsigned)std::min<uint32_t>((uint32_t)num_sms(), nblocks);
     kern<<<grid, 32 * (1 + kAcc) + 128 * epi, smem, st>>>(s->maps.cand, s->maps.query, a);
     HJ_LAUNCHED();
@@ -1114,8 +1134,8 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
 
 hj_status launch_band_recheck(const hj_index* ix, const uint32_t* bq, const uint32_t* bc,
                               const unsigned long long* band_used, unsigned long long band_cap, const PairSink& sink,
-                              cudaStream_t st) {
-    unsigned grid = (unsigned)num_sms() * 8;
+                              uint32_t nblocks, cudaStream_t st) {
+    const unsigned grid = recheck_grid(nblocks);
     k_band_recheck<<<grid, 256, 0, st>>>((const float*)ix->pts, ix->perm, ix->d, (float)ix->thr, bq, bc, band_used,
                                          band_cap, sink);
     HJ_LAUNCHED();
@@ -1124,23 +1144,25 @@ hj_status launch_band_recheck(const hj_index* ix, const uint32_t* bq, const uint
 
 }  // namespace hj
 
-extern "C" hj_status hj_probe_tc_tile(hj_index* ix, int kind, uint32_t a0, uint32_t b0, float* d_out,
-                                      void* h_query_rows, void* h_cand_rows, void* stream) {
-    using namespace hj;
-    if (!ix || !d_out || !tc_supported(ix, kind)) { set_error("hj_probe_tc_tile: unsupported"); return HJ_ERR_INVALID; }
-    cudaStream_t st = as_stream(stream);
+namespace hj {
+// One launch of the tile probe.  skip_mma = 1 issues the loads but no MMA and no
+// commit, so the epilogue's bounded wait runs out after wait_cycles.
+static hj_status run_tile_probe(hj_index* ix, int kind, uint32_t a0, uint32_t b0, float* d_out, uint32_t skip_mma,
+                                long long wait_cycles, void* h_query_rows, void* h_cand_rows, cudaStream_t st) {
+    if (!ix || !d_out || !tc_supported(ix, kind)) { set_error("tensor-core tile probe: unsupported"); return HJ_ERR_INVALID; }
     HJ_TRY(tc_prepare(ix, kind, st));
     TcState* s = tc_state(ix);
     const uint32_t nkb = ix->tc_kpad / 32;
     size_t smem = 1024 + (size_t)(kQT + 1) * nkb * kKBlockBytes + 64;
     smem = std::max<size_t>(smem, 116 * 1024);
     HJ_TRY(ensure_smem(k_tc_tile_probe, smem));
+    Scratch tmp(st);
     uint32_t* err = nullptr;
-    HJ_TRY(dalloc(&err, 1, st));
+    HJ_TRY(tmp.alloc(&err, 1));
     HJ_CUDA(cudaMemsetAsync(err, 0, 4, st));
     k_tc_tile_probe<<<1, kProbeThreads, smem, st>>>(s->maps.cand, s->maps.query, nkb,
                                                tc::idesc_f16(kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kAccCols),
-                                               a0, b0, d_out, err);
+                                               a0, b0, d_out, err, skip_mma, wait_cycles);
     HJ_LAUNCHED();
     uint32_t herr = 0;
     HJ_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
@@ -1152,9 +1174,29 @@ extern "C" hj_status hj_probe_tc_tile(hj_index* ix, int kind, uint32_t a0, uint3
                                 (size_t)std::min<uint32_t>(kTileRows, ix->n - a0) * ix->tc_kpad * 2,
                                 cudaMemcpyDeviceToHost, st));
     HJ_CUDA(cudaStreamSynchronize(st));
-    dfree(err, st);
-    if (herr) { set_error("hj_probe_tc_tile: a bounded wait expired"); return HJ_ERR_TIMEOUT; }
+    if (herr) { set_error("tensor-core tile probe: a bounded wait expired"); return HJ_ERR_TIMEOUT; }
     return HJ_OK;
+}
+}  // namespace hj
+
+extern "C" hj_status hj_probe_tc_tile(hj_index* ix, int kind, uint32_t a0, uint32_t b0, float* d_out,
+                                      void* h_query_rows, void* h_cand_rows, void* stream) {
+    using namespace hj;
+    if (ix && (a0 >= ix->n || b0 >= ix->n)) { set_error("hj_probe_tc_tile: row out of range"); return HJ_ERR_INVALID; }
+    return run_tile_probe(ix, kind, a0, b0, d_out, 0u, kWaitCycles, h_query_rows, h_cand_rows, as_stream(stream));
+}
+
+extern "C" hj_status hj_probe_tc_wait_timeout(hj_index* ix, int kind, uint64_t wait_cycles, void* stream) {
+    using namespace hj;
+    if (!ix || wait_cycles == 0 || wait_cycles > (uint64_t)kWaitCycles) {
+        set_error("hj_probe_tc_wait_timeout: wait_cycles must be in [1, %lld]", kWaitCycles);
+        return HJ_ERR_INVALID;
+    }
+    cudaStream_t st = as_stream(stream);
+    Scratch tmp(st);
+    float* out = nullptr;
+    HJ_TRY(tmp.alloc(&out, (size_t)kTileRows * kQB));
+    return run_tile_probe(ix, kind, 0, 0, out, 1u, (long long)wait_cycles, nullptr, nullptr, st);
 }
 
 extern "C" hj_status hj_tc_operand_scale(const hj_index* ix, int* log2_scale) {

@@ -110,15 +110,15 @@ template <typename In, typename Out>
 hj_status exclusive_scan(const In* in, Out* out, uint64_t n, cudaStream_t st) {
     if (n == 0) return HJ_OK;
     uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    Scratch tmp(st);
     Out* sums = nullptr;
-    HJ_TRY(dalloc(&sums, tiles, st));
+    HJ_TRY(tmp.alloc(&sums, tiles));
     k_tile_sums<In, Out><<<(unsigned)tiles, kScanBlock, 0, st>>>(in, n, sums);
     HJ_LAUNCHED();
     k_scan_sums<Out><<<1, kScanBlock, 0, st>>>(sums, tiles);
     HJ_LAUNCHED();
     k_scan_tiles<In, Out><<<(unsigned)tiles, kScanBlock, 0, st>>>(in, out, n, sums);
     HJ_LAUNCHED();
-    dfree(sums, st);
     return HJ_OK;
 }
 
@@ -201,8 +201,9 @@ hj_status radix_sort(K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, u
         return HJ_ERR_INVALID;
     }
     uint32_t ntiles = (uint32_t)((n + kRsTile - 1) / kRsTile);
+    Scratch tmp(st);
     uint32_t* hist = nullptr;
-    HJ_TRY(dalloc(&hist, (size_t)kRadix * ntiles, st));
+    HJ_TRY(tmp.alloc(&hist, (size_t)kRadix * ntiles));
     K* src_k = keys; uint32_t* src_v = vals;
     K* dst_k = keys_tmp; uint32_t* dst_v = vals_tmp;
     uint32_t passes = (nbits + 7) / 8;
@@ -220,7 +221,6 @@ hj_status radix_sort(K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, u
         HJ_CUDA(cudaMemcpyAsync(keys, src_k, n * sizeof(K), cudaMemcpyDeviceToDevice, st));
         HJ_CUDA(cudaMemcpyAsync(vals, src_v, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     }
-    dfree(hist, st);
     return HJ_OK;
 }
 

@@ -99,7 +99,7 @@ typedef struct {
     uint32_t max_batches;          /* safety cap on batch count; 0 = unlimited */
     uint32_t use_graphs;           /* reserved, ignored: a batch is a handful of launches */
     uint32_t keep_keys;            /* keep per-batch sorted key arrays (needed for the reference export) */
-    uint32_t shard_count;          /* multi-GPU: work items i with i % shard_count == shard_index (0 = all) */
+    uint32_t shard_count;          /* multi-GPU: this rank's LPT share of the work items (0 or 1 = all) */
     uint32_t shard_index;
 } hj_join_opts;
 
@@ -116,6 +116,7 @@ typedef struct {
     uint32_t refine_launches;      /* refine kernel launches timed in ms_refine_kernel */
     uint32_t refine_used;          /* HJ_REFINE_* actually used */
     uint32_t kernel_launches;      /* kernels launched by this join */
+    float ms_setup;                /* workload order, refine choice, operand forms, work items (wall clock) */
 } hj_join_stats;
 
 /* ---- errors / library ---------------------------------------------------- */
@@ -123,6 +124,23 @@ const char* hj_last_error(void);
 const char* hj_version(void);
 /* Kernels launched by this process so far (all entry points). */
 uint64_t hj_kernel_launch_count(void);
+
+/* ---- dataset ingest: replaces importNDDataset (import_dataset.cpp:10-40) ---- */
+/* Parses a text dataset the way the reference's importer does: the file split
+ * into tokens at every ',', values extracted from each token as
+ * `stringstream >> DTYPE` would (whitespace skipped, the C-locale number
+ * grammar, strtof/strtod rounding), a token's remainder dropped after the
+ * first failed extraction, and the trailing values that do not fill a point of
+ * d coordinates dropped.  The file is parsed in parallel (OpenMP) with the same
+ * values in the same order.  *h_values receives n_points x d values of the
+ * dataset type, allocated by the library: release it with hj_host_free. */
+hj_status hj_import_text(const char* path, uint32_t d, int dtype, void** h_values, uint64_t* n_points);
+/* The binary twin: a 32-byte header ("HJDS0001", dtype, d, n) and the values.
+ * hj_import_binary also reads the reference's raw layout (importNDDatasetBinary,
+ * import_dataset.cpp:63-100: values only, n from the file size). */
+hj_status hj_write_binary(const char* path, const void* h_values, uint64_t n_points, uint32_t d, int dtype);
+hj_status hj_import_binary(const char* path, uint32_t d, int dtype, void** h_values, uint64_t* n_points);
+void hj_host_free(void* p);
 
 /* ---- grid geometry: replaces generateNDGridDimensions (main.cu:449-520) ---- */
 /* Per indexed dimension: min/max over the points, widened by eps, nCells =
@@ -204,12 +222,48 @@ hj_status hj_result_to_csr(const hj_result* r, uint64_t* d_offsets, uint32_t* d_
 hj_status hj_result_digest(const hj_result* r, uint32_t* d_count, uint64_t* d_sum, uint64_t* d_xor,
                            void* stream);
 
+/* ---- streamed join: results larger than device memory ----------------------- */
+/* One grouped batch handed to a sink: `count` pairs, query ids ascending in
+ * d_keys and their neighbour ids in d_vals (device memory, in the order of the
+ * join's stream).  The reference's counterpart is the per-batch copy-out and
+ * host table build of distanceTableNDGridBatches (GPU.cu:1542-1573). */
+typedef struct {
+    uint32_t batch;                /* 0, 1, ... in the order the batches complete */
+    uint32_t pad_;
+    uint64_t count;
+    const uint32_t* d_keys;
+    const uint32_t* d_vals;
+} hj_batch_view;
+/* Called on the joining thread once per batch.  The arrays stay valid for work
+ * the sink enqueues on `stream` (copies, kernels): the next batch reuses them
+ * only after that work, in stream order.  Return HJ_OK to continue; any other
+ * status stops the join and is returned by hj_join_stream. */
+typedef hj_status (*hj_batch_sink)(const hj_batch_view* batch, void* user, void* stream);
+
+/* The join of hj_join with nothing kept on the device: each batch is grouped by
+ * query id and handed to `sink` (may be NULL), and its buffers are reused by
+ * the next batch, so the result may exceed device memory.  When d_count, d_sum
+ * and d_xor (n entries each, device) are given they receive the per-query
+ * digest of hj_result_digest, accumulated over the batches (they are zeroed
+ * first).  Synchronises `stream`. */
+hj_status hj_join_stream(hj_index* ix, const hj_join_opts* opts, hj_batch_sink sink, void* user,
+                         uint32_t* d_count, uint64_t* d_sum, uint64_t* d_xor, void* stream,
+                         hj_join_stats* stats);
+
 /* ---- multi-GPU sharding ----------------------------------------------------- */
 /* The work items a rank processes out of `n_items` heaviest-first items when
  * the join runs with shard_count ranks: items first, first + stride, ... (n_mine
  * of them).  Host-only arithmetic; hj_join applies exactly this selection. */
 hj_status hj_shard_plan(uint32_t n_items, uint32_t shard_count, uint32_t shard_index, uint32_t* first,
                         uint32_t* stride, uint32_t* n_mine);
+/* The items a rank processes under greedy LPT (longest processing time first):
+ * items by cost, descending (ties by index), each to the least-loaded rank
+ * (ties to the lowest rank).  Writes this rank's item indices, ascending, to
+ * items (capacity n_items) and their number to n_mine.  Host-only arithmetic;
+ * hj_join with shard_count > 1 applies it with cost = candidates x queries per
+ * work item, so every rank derives the same partition. */
+hj_status hj_shard_plan_lpt(const uint64_t* costs, uint32_t n_items, uint32_t shard_count, uint32_t shard_index,
+                            uint32_t* items, uint32_t* n_mine);
 
 /* ---- one-shot convenience: host buffers in, host pair count out ------------ */
 /* Copies the dataset to the device, builds the index, sorts by workload and
@@ -248,6 +302,15 @@ hj_status hj_server_wait(hj_server* s, uint64_t ticket, double timeout_s, hj_res
                          hj_serve_info* info);
 hj_status hj_server_destroy(hj_server* s);
 
+/* ---- fault injection and accounting for tests --------------------------------- */
+/* Arms the library's device-allocation fault injection: the nth device
+ * allocation from now (n >= 1) fails as an out-of-memory would; 0 disarms.
+ * No reference counterpart: it exercises every error path's clean-up. */
+void hj_debug_fail_alloc(uint64_t nth);
+/* Bytes currently allocated from the device's default memory pool (the pool
+ * every stream-ordered allocation of the library comes from). */
+hj_status hj_debug_pool_used(uint64_t* bytes);
+
 /* ---- probes --------------------------------------------------------------- */
 /* Evaluates the reference's squared-distance expression (kernel.cu:350-353)
  * as nvcc compiles it by default, for n pairs of d-dimensional rows; writes
@@ -265,6 +328,14 @@ hj_status hj_probe_sqdist(const void* d_a, const void* d_b, uint32_t n, uint32_t
  * by 2^s and accumulators by 4^s, s from hj_tc_operand_scale. */
 hj_status hj_probe_tc_tile(hj_index* ix, int refine_kind, uint32_t a0, uint32_t b0, float* d_out,
                            void* h_query_rows, void* h_cand_rows, void* stream);
+
+/* Failure-detection check of the tensor-core pipeline's bounded waits: one tile
+ * probe launch whose MMA issuer issues neither MMAs nor their commit (after its
+ * operand loads have landed), so the epilogue's wait on the commit barrier runs
+ * out after wait_cycles SM cycles.  The kernel then raises its error flag,
+ * releases its tensor memory and returns; the call returns HJ_ERR_TIMEOUT and
+ * the context stays usable.  No reference counterpart. */
+hj_status hj_probe_tc_wait_timeout(hj_index* ix, int refine_kind, uint64_t wait_cycles, void* stream);
 
 /* The power-of-two exponent s of the tensor-core operand forms last prepared
  * for this index: they hold (x - min) * 2^s, chosen per dataset so that every

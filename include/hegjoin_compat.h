@@ -58,4 +58,10 @@ void constructNeighborTableKeyValueWithPtrs(int* pointIDKey, int* pointInDistVal
 /* GPU.h:97 */
 void warmUpGPU();
 
+/* main.h:9-16, implemented in hegjoin_b200/compat/hegjoin_import.cpp (link it in
+ * place of import_dataset.cpp): the same text and raw-binary formats and the same
+ * values, parsed by the library's parallel importer (hj_import_text). */
+void importNDDataset(std::vector<std::vector<DTYPE> >* dataPoints, char* fname);
+void importNDDatasetBinary(std::vector<std::vector<DTYPE> >* dataPoints, char* fname);
+
 #endif /* HEGJOIN_COMPAT_H */

@@ -42,6 +42,11 @@ def _load():
         getattr(lib, f"hjo_join_lists_{suf}").restype = U64
         getattr(lib, f"hjo_sqdist_{suf}").argtypes = [P, P, U32, I]
         getattr(lib, f"hjo_sqdist_{suf}").restype = D
+    for suf in ("f32", "f64"):
+        getattr(lib, f"hjo_import_text_{suf}").argtypes = [ctypes.c_char_p, P, U64]
+        getattr(lib, f"hjo_import_text_{suf}").restype = U64
+    lib.hjo_write_text.argtypes = [ctypes.c_char_p, P, U64, U32, I, I]
+    lib.hjo_write_text.restype = I
     lib.hjo_ref_cell_order.argtypes = [P, U32, P]
     lib.hjo_ref_cell_order.restype = None
     lib.hjo_digest.argtypes = [P, P, U32, P, P]
@@ -236,6 +241,24 @@ def ref_batches(counts: np.ndarray, origin: np.ndarray):
     csum = np.concatenate([[0], np.cumsum(per_q)])
     actual = [int(csum[b] - csum[a]) for a, b in batches]
     return buf, batches, actual
+
+
+def write_text(path: str, db: np.ndarray, digits: int) -> None:
+    """The reference generator's text layout ("v, v, ..., v" lines), `digits` significant digits."""
+    db = np.ascontiguousarray(db)
+    if lib.hjo_write_text(path.encode(), db.ctypes.data, db.shape[0], db.shape[1], int(db.dtype == np.float64),
+                          digits) != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def import_text(path: str, dtype) -> np.ndarray:
+    """import_dataset.cpp:10-40 restated: every value the file holds, in order (flat)."""
+    suf = "f32" if np.dtype(dtype) == np.float32 else "f64"
+    fn = getattr(lib, f"hjo_import_text_{suf}")
+    n = fn(path.encode(), None, 0)
+    out = np.zeros(max(1, n), dtype=dtype)
+    fn(path.encode(), out.ctypes.data, n)
+    return out[:n]
 
 
 def num_threads() -> int:

@@ -23,7 +23,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
 #include <vector>
 #include <omp.h>
 
@@ -139,6 +143,25 @@ void for_each_stencil_cell(const T* p, uint32_t k, T eps, const T* minArr, const
     }
 }
 
+// import_dataset.cpp:10-40 (importNDDataset), restated with the same standard
+// library calls: tokens from getline(in, f, ','), values from a stringstream
+// over each token with `>>` until an extraction fails.  Writes at most
+// `capacity` values to out and returns how many the file holds.
+template <typename T>
+uint64_t import_text(const char* path, T* out, uint64_t capacity) {
+    std::ifstream in(path);
+    uint64_t cnt = 0;
+    for (std::string f; std::getline(in, f, ',');) {
+        T v;
+        std::stringstream ss(f);
+        while (ss >> v) {
+            if (cnt < capacity) out[cnt] = v;
+            ++cnt;
+            if (ss.peek() == ',') ss.ignore();
+        }
+    }
+    return cnt;
+}
 inline uint64_t mix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ull;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -321,6 +344,31 @@ HJO_JOIN_SAMPLE(double, f64)
     }
 HJO_JOIN_LISTS(float, f32)
 HJO_JOIN_LISTS(double, f64)
+
+// The reference generator's text layout (datasets/dataset_gen_fixed_len_expo_dist.cpp:
+// 76-83: "v, v, ..., v" per line) with `digits` significant digits per value, for
+// ingest tests and timings.  Returns 0 on success.
+int hjo_write_text(const char* path, const void* vals, uint64_t n, uint32_t d, int is_double, int digits) {
+    FILE* f = std::fopen(path, "w");
+    if (!f) return 1;
+    std::vector<char> buf(1 << 20);
+    std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+    for (uint64_t i = 0; i < n; ++i) {
+        for (uint32_t j = 0; j < d; ++j) {
+            const double v = is_double ? static_cast<const double*>(vals)[i * d + j]
+                                       : (double)static_cast<const float*>(vals)[i * d + j];
+            std::fprintf(f, j + 1 < d ? "%.*g, " : "%.*g\n", digits, v);
+        }
+    }
+    return std::fclose(f) != 0;
+}
+
+uint64_t hjo_import_text_f32(const char* path, float* out, uint64_t capacity) {
+    return import_text<float>(path, out, capacity);
+}
+uint64_t hjo_import_text_f64(const char* path, double* out, uint64_t capacity) {
+    return import_text<double>(path, out, capacity);
+}
 
 // Squared distance of one pair in the reference order (for error statistics).
 double hjo_sqdist_f32(const float* a, const float* b, uint32_t d, int fma_mode) {

@@ -4,8 +4,10 @@
 // distanceTableNDGridBatches -- here resolved by hegjoin_b200's compatibility
 // shim -- and writes the neighbour table as per-query sorted lists.
 //
-// usage: compat_main dataset.bin eps out.bin
-//   dataset.bin: u32 n, u32 d, u32 sizeof(value), then n*d values.
+// usage: compat_main dataset eps out.bin
+//   dataset: u32 n, u32 d, u32 sizeof(value), then n*d values; or, when the
+//   name ends in ".txt", the reference's text format, read with importNDDataset
+//   (main.cu:89) as main does.
 //   out.bin: u64 totalNeighbors, u64 totalCandidates, u32 nNonEmptyCells,
 //            (n + 1) u64 offsets, neighbour ids (u32).
 #include <algorithm>
@@ -13,6 +15,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -22,15 +25,25 @@
 #include "hegjoin_compat.h"
 
 int main(int argc, char** argv) {
-    if (argc != 4) { fprintf(stderr, "usage: %s dataset.bin eps out.bin\n", argv[0]); return 1; }
-    FILE* f = fopen(argv[1], "rb");
-    if (!f) { perror(argv[1]); return 1; }
-    uint32_t hdr[3];
-    if (fread(hdr, 4, 3, f) != 3 || hdr[1] != GPUNUMDIM || hdr[2] != sizeof(DTYPE)) { fprintf(stderr, "bad dataset\n"); return 1; }
-    unsigned int DBSIZE = hdr[0];
-    std::vector<DTYPE> db((size_t)DBSIZE * GPUNUMDIM);
-    if (fread(db.data(), sizeof(DTYPE), db.size(), f) != db.size()) { fprintf(stderr, "short read\n"); return 1; }
-    fclose(f);
+    if (argc != 4) { fprintf(stderr, "usage: %s dataset eps out.bin\n", argv[0]); return 1; }
+    std::string name = argv[1];
+    unsigned int DBSIZE = 0;
+    std::vector<DTYPE> db;
+    if (name.size() > 4 && name.compare(name.size() - 4, 4, ".txt") == 0) {
+        std::vector<std::vector<DTYPE> > pts;
+        importNDDataset(&pts, argv[1]);
+        DBSIZE = (unsigned int)pts.size();
+        for (const auto& p : pts) db.insert(db.end(), p.begin(), p.end());
+    } else {
+        FILE* f = fopen(argv[1], "rb");
+        if (!f) { perror(argv[1]); return 1; }
+        uint32_t hdr[3];
+        if (fread(hdr, 4, 3, f) != 3 || hdr[1] != GPUNUMDIM || hdr[2] != sizeof(DTYPE)) { fprintf(stderr, "bad dataset\n"); return 1; }
+        DBSIZE = hdr[0];
+        db.resize((size_t)DBSIZE * GPUNUMDIM);
+        if (fread(db.data(), sizeof(DTYPE), db.size(), f) != db.size()) { fprintf(stderr, "short read\n"); return 1; }
+        fclose(f);
+    }
     DTYPE epsilon = atof(argv[2]);
 
     // grid geometry as main.cu:449-520 computes it

@@ -13,7 +13,8 @@ LIBS = {"hegjoin_b200.h": "libhegjoin_b200.so", "hegjoin_datagen.h": "libhj_data
 def _declared(header):
     src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return {m.group(1) for m in re.finditer(r"\b(hj_\w+)\s*\(", src)}
+    # function declarations: a name followed by "(", not a function-pointer typedef "(*"
+    return {m.group(1) for m in re.finditer(r"\b(hj_\w+)\s*\((?!\s*\*)", src)}
 
 
 def test_library_exports_declared_symbols():

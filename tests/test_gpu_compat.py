@@ -22,15 +22,23 @@ def _exe(cfg):
     return os.path.join(ROOT, "_build", "compat", cfg, "compat_main")
 
 
+@pytest.mark.parametrize("text", [False, True])
 @pytest.mark.parametrize("cfg,n,seed,eps", [("d18", 6000, 61, 0.07), ("d2", 8000, 62, 0.006)])
-def test_reference_signatures_end_to_end(cuda, tmp_path, cfg, n, seed, eps):
+def test_reference_signatures_end_to_end(cuda, tmp_path, cfg, n, seed, eps, text):
     d, k, t = BUILDS[cfg]
     dt = np.float32 if t == "float" else np.float64
     db = workloads.exp40(seed, n, d, dt)
-    path = tmp_path / "db.bin"
-    with open(path, "wb") as f:
-        np.array([n, d, db.dtype.itemsize], np.uint32).tofile(f)
-        db.tofile(f)
+    if text:
+        # the reference generator's text format, read back by the importer shim (importNDDataset)
+        path = tmp_path / "db.txt"
+        with open(path, "w") as f:
+            for row in db:
+                f.write(", ".join("%.17g" % float(v) for v in row) + "\n")
+    else:
+        path = tmp_path / "db.bin"
+        with open(path, "wb") as f:
+            np.array([n, d, db.dtype.itemsize], np.uint32).tofile(f)
+            db.tofile(f)
     out = tmp_path / "out.bin"
     p = subprocess.run([_exe(cfg), str(path), repr(float(eps)), str(out)], capture_output=True, text=True,
                        timeout=600)

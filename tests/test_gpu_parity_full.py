@@ -7,6 +7,9 @@ whole dataset: the heaviest 300 and the lightest 700 of the workload order,
 700 around its median, and 300 at random.  Counts and sorted lists must match
 bit for bit under the default refine and the exact one.
 """
+import hashlib
+import json
+import os
 import time
 
 import numpy as np
@@ -73,4 +76,38 @@ def test_full_size_sampled_lists_match_oracle(cuda, name, refines):
         res.close()
     assert len(set(totals.values())) == 1
     print(f"{name}: oracle sample {t_oracle:.1f} s")
+    ix.close()
+
+
+def test_c1_full_size_streamed_matches_oracle(cuda):
+    """The 2-D FP64 configuration at 2,000,000 points (about 1.9e10 pairs, more than
+    device memory holds) through the streamed join: every query's neighbour count
+    equals the oracle's, and sampled queries' digests equal those of the oracle's
+    neighbour lists."""
+    import torch
+    import hegjoin_b200 as hj
+    wl = workloads.WORKLOADS["c1_2d"]
+    db = wl.generate()
+    ix = hj.GridIndex(torch.from_numpy(db).to(cuda), wl.k, wl.eps)
+    ix.sort_by_workload()
+    _, origin = ix.workload_export()
+    qids = _sample_queries(origin.cpu().numpy().astype(np.uint32), seed=wl.seed)
+    st, (c, s, x) = hj.join_stream(ix, None, digest=True, refine="exact")
+    assert st.n_batches > 1
+    # all 2M counts against the oracle's count pass (tests/golden/make_c1_counts.py)
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "c1_2d_counts.json")))
+    assert (gold["n"], gold["eps"], gold["seed"]) == (wl.n, wl.eps, wl.seed)
+    counts = c.cpu().numpy().astype("<u4")
+    assert st.total_pairs == gold["total_pairs"]
+    assert hashlib.sha256(counts.tobytes()).hexdigest() == gold["counts_sha256"]
+    mn, _, nc, _ = oracle.geometry(db, wl.k, wl.eps)
+    sc, lists = oracle.join_lists(db, wl.k, wl.eps, qids, mn, nc)
+    soff = np.zeros(len(qids) + 1, np.uint64)
+    np.cumsum(sc, out=soff[1:])
+    _, osum, oxor = oracle.digest(soff, lists)
+    q = torch.from_numpy(qids.astype(np.int64)).to(cuda)
+    assert np.array_equal(s[q].cpu().numpy().view(np.uint64), osum)
+    assert np.array_equal(x[q].cpu().numpy().view(np.uint64), oxor)
+    print(f"c1_2d: {st.total_pairs} pairs in {st.n_batches} batches; all {len(db)} counts and "
+          f"{len(qids)} sampled digests match the oracle")
     ix.close()

@@ -68,3 +68,55 @@ def test_shard_plan_rejects_bad_index():
     import hegjoin_b200 as hj
     with pytest.raises(hj.HJError):
         hj.shard_plan(10, 2, 2)
+
+
+# ---- greedy LPT: the partition hj_join applies with shard_count > 1 ---------------------------
+def _lpt_rank(rank, world, port, costs, q):
+    import numpy as np
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import hegjoin_b200 as hj
+    mine = hj.shard_plan_lpt(np.array(costs, np.uint64), world, rank).tolist()
+    parts = [None] * world
+    dist.all_gather_object(parts, mine)
+    if rank == 0:
+        q.put(parts)
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_lpt_ranks_partition_items_and_balance(world):
+    import numpy as np
+    rng = np.random.default_rng(world)
+    costs = (rng.pareto(1.2, 500) * 1000).astype(np.uint64).tolist()   # skewed item costs
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_lpt_rank, args=(r, world, port, costs, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(120)
+        assert p.exitcode == 0
+    parts = q.get(timeout=10)
+    assert sorted(i for p in parts for i in p) == list(range(len(costs)))     # every item exactly once
+    loads = [sum(costs[i] for i in p) for p in parts]
+    # Graham's bound for LPT: the largest load is within max(cost) of the mean
+    assert max(loads) - sum(loads) / world <= max(costs)
+    for p in parts:
+        assert p == sorted(p)
+
+
+def test_lpt_plan_cases():
+    import numpy as np
+    import hegjoin_b200 as hj
+    c = np.array([5, 4, 3, 3, 2, 1], np.uint64)
+    assert hj.shard_plan_lpt(c, 2, 0).tolist() == [0, 3, 5]
+    assert hj.shard_plan_lpt(c, 2, 1).tolist() == [1, 2, 4]
+    assert hj.shard_plan_lpt(np.zeros(0, np.uint64), 2, 1).tolist() == []
+    assert hj.shard_plan_lpt(c, 1, 0).tolist() == list(range(6))
+    assert hj.shard_plan_lpt(c, 8, 7).tolist() == []                  # more ranks than items
+    with pytest.raises(hj.HJError):
+        hj.shard_plan_lpt(c, 2, 2)
