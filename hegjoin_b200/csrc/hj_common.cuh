@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -9,6 +10,7 @@
 #include <vector>
 
 #include "hegjoin_b200.h"
+#include "hj_workspace.h"
 
 namespace hj {
 
@@ -70,6 +72,7 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // Fault injection for tests (hj_debug_fail_alloc): while armed with n > 0, the
 // n-th dalloc from then on fails the way an out-of-memory would.
 bool injected_alloc_failure();   // hj_index.cu
+bool injected_alloc_failure_armed();
 
 // Stream-ordered device allocation; freed with dfree on the same stream.
 template <typename T>
@@ -97,26 +100,50 @@ void dfree(T*& p, cudaStream_t st) {
 
 // The device temporaries of one call: everything allocated through the guard is
 // freed (in the order of its stream) when the guard goes out of scope, on every
-// return path, unless it was handed over with keep().
+// return path, unless it was handed over with keep() (pool blocks only: use
+// alloc_pool for a buffer that will outlive the guard).
 class Scratch {
   public:
-    explicit Scratch(cudaStream_t st) : st_(st) {}
+    explicit Scratch(cudaStream_t st) : st_(st), ws_(current_workspace()) {
+        if (ws_ && ws_->stream != st) ws_ = nullptr;
+        if (ws_) {
+            mark_ = ws_->top;
+            depth_ = ++ws_->depth;
+        }
+    }
     Scratch(const Scratch&) = delete;
     Scratch& operator=(const Scratch&) = delete;
     ~Scratch() {
         for (void* p : held_) cudaFreeAsync(p, st_);
+        if (ws_) {
+            ws_->top = mark_;
+            --ws_->depth;
+        }
     }
     template <typename T>
     hj_status alloc(T** p, size_t count) {
+        if (ws_ && depth_ == ws_->depth && !injected_alloc_failure_armed()) {
+            const size_t bytes = ((std::max<size_t>(count, 1) * sizeof(T)) + 255) & ~size_t(255);
+            if (ws_->top + bytes <= ws_->cap) {
+                *p = reinterpret_cast<T*>(ws_->base + ws_->top);
+                ws_->top += bytes;
+                return HJ_OK;
+            }
+        }
+        return alloc_pool(p, count);
+    }
+    template <typename T>
+    hj_status alloc_pool(T** p, size_t count) {
         hj_status s = dalloc(p, count, st_);
         if (s == HJ_OK) held_.push_back(*p);
         return s;
     }
-    // Free one temporary now (its memory goes back to the pool for the next allocation).
+    // Free one temporary now (a pool block goes back to the pool for the next
+    // allocation; a workspace block is given back when the guard ends).
     template <typename T>
     void release(T*& p) {
-        drop(p);
-        dfree(p, st_);
+        if (drop(p)) dfree(p, st_);
+        p = nullptr;
     }
     // Hand a buffer to a longer-lived owner: the guard no longer frees it.
     template <typename T>
@@ -132,15 +159,19 @@ class Scratch {
     }
 
   private:
-    void drop(const void* p) {
+    bool drop(const void* p) {
         for (size_t i = 0; i < held_.size(); ++i)
             if (held_[i] == p) {
                 held_[i] = held_.back();
                 held_.pop_back();
-                return;
+                return true;
             }
+        return false;
     }
     cudaStream_t st_;
+    Workspace* ws_ = nullptr;
+    size_t mark_ = 0;
+    uint32_t depth_ = 0;
     std::vector<void*> held_;
 };
 

@@ -43,7 +43,12 @@ void count_launch() {
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 uint64_t thread_launch_count() { return t_launches; }
 
+static thread_local Workspace* t_workspace = nullptr;
+Workspace* current_workspace() { return t_workspace; }
+void set_current_workspace(Workspace* ws) { t_workspace = ws; }
+
 static std::atomic<int64_t> g_fail_alloc_in{0};
+bool injected_alloc_failure_armed() { return g_fail_alloc_in.load(std::memory_order_relaxed) > 0; }
 bool injected_alloc_failure() {
     if (g_fail_alloc_in.load(std::memory_order_relaxed) <= 0) return false;
     return g_fail_alloc_in.fetch_sub(1, std::memory_order_relaxed) == 1;
@@ -118,28 +123,34 @@ __device__ __forceinline__ uint32_t cell_coord(double x, double mn, double eps) 
 
 // ---- geometry: per-dimension min / max ----------------------------------------------
 template <typename T>
-__global__ void k_minmax(const T* __restrict__ db, uint32_t n, uint32_t d, uint32_t j, T* out_min, T* out_max) {
+__global__ void k_minmax(const T* __restrict__ db, uint32_t n, uint32_t d, uint32_t k, T* out_min, T* out_max) {
+    // per block: the minimum and maximum of each of the k indexed dimensions, all
+    // dimensions in one launch (partials [dim][block])
     __shared__ T smin[32], smax[32];
-    T mn = db[j], mx = db[j];
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        T v = db[i * d + j];
-        mn = v < mn ? v : mn;
-        mx = v > mx ? v : mx;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        T a = __shfl_down_sync(0xffffffffu, mn, o), b = __shfl_down_sync(0xffffffffu, mx, o);
-        mn = a < mn ? a : mn;
-        mx = b > mx ? b : mx;
-    }
-    if (lane_id() == 0) { smin[threadIdx.x >> 5] = mn; smax[threadIdx.x >> 5] = mx; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-            mn = smin[w] < mn ? smin[w] : mn;
-            mx = smax[w] > mx ? smax[w] : mx;
+    for (uint32_t j = 0; j < k; ++j) {
+        T mn = db[j], mx = db[j];
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += (uint64_t)gridDim.x * blockDim.x) {
+            T v = db[i * d + j];
+            mn = v < mn ? v : mn;
+            mx = v > mx ? v : mx;
         }
-        out_min[blockIdx.x] = mn;
-        out_max[blockIdx.x] = mx;
+        for (int o = 16; o > 0; o >>= 1) {
+            T a = __shfl_down_sync(0xffffffffu, mn, o), b = __shfl_down_sync(0xffffffffu, mx, o);
+            mn = a < mn ? a : mn;
+            mx = b > mx ? b : mx;
+        }
+        if (lane_id() == 0) { smin[threadIdx.x >> 5] = mn; smax[threadIdx.x >> 5] = mx; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+                mn = smin[w] < mn ? smin[w] : mn;
+                mx = smax[w] > mx ? smax[w] : mx;
+            }
+            out_min[(size_t)j * gridDim.x + blockIdx.x] = mn;
+            out_max[(size_t)j * gridDim.x + blockIdx.x] = mx;
+        }
+        __syncthreads();
     }
 }
 
@@ -150,10 +161,8 @@ hj_status geometry_t(const T* db, uint32_t n, uint32_t d, uint32_t k, T eps, dou
     Scratch tmp(st);
     T* part = nullptr;
     HJ_TRY(tmp.alloc(&part, (size_t)2 * blocks * k));
-    for (uint32_t j = 0; j < k; ++j) {
-        k_minmax<T><<<blocks, 256, 0, st>>>(db, n, d, j, part + (size_t)j * blocks, part + (size_t)(k + j) * blocks);
-        HJ_LAUNCHED();
-    }
+    k_minmax<T><<<blocks, 256, 0, st>>>(db, n, d, k, part, part + (size_t)k * blocks);
+    HJ_LAUNCHED();
     std::vector<T> hp((size_t)2 * blocks * k);
     HJ_CUDA(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(T), cudaMemcpyDeviceToHost, st));
     HJ_CUDA(cudaStreamSynchronize(st));
@@ -476,7 +485,7 @@ hj_status build_blocks(const hj_index* ix, uint32_t qb, HjBlock** d_blocks, uint
     HJ_CUDA(cudaMemcpyAsync(&nb, cnt + nC, 4, cudaMemcpyDeviceToHost, st));
     HJ_CUDA(cudaStreamSynchronize(st));
     HjBlock* blocks = nullptr;
-    HJ_TRY(tmp.alloc(&blocks, (size_t)std::max<uint32_t>(nb, 1)));
+    HJ_TRY(tmp.alloc_pool(&blocks, (size_t)std::max<uint32_t>(nb, 1)));   // handed to the caller
     k_make_blocks<<<g, 256, 0, st>>>(ix->cell_order, ix->cell_start, ix->cell_nb, cnt, nC, qb, blocks);
     HJ_LAUNCHED();
     *d_blocks = tmp.keep(blocks);

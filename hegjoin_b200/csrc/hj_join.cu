@@ -78,6 +78,30 @@ __global__ void k_pick_samples(const HjBlock* __restrict__ blocks, uint32_t nblo
     out[i] = blocks[min(nblocks - 1, i * stride)];
 }
 
+// Counters and flags of one join, in one device allocation.
+struct JoinCtl {
+    unsigned long long cursor;        // pair sink cursor of the current batch
+    unsigned long long valid;         // pairs left after grouping (sentinels dropped)
+    unsigned long long tc_acc;        // tensor-core filter: pairs accepted outside the band
+    unsigned long long tc_band;       // tensor-core filter: band pairs
+    unsigned long long band_cursor;   // band sink cursor of the current batch
+    uint32_t head;                    // work-item queue head of the current launch
+    uint32_t overflow;                // a sink ran out of room
+    uint32_t timeout;                 // a bounded device-side wait expired
+    uint32_t pad_;
+};
+
+// Start of a batch: both sink cursors, the overflow flag and the queue head.
+__global__ void k_batch_reset(JoinCtl* c) {
+    if (threadIdx.x == 0) {
+        c->cursor = 0;
+        c->band_cursor = 0;
+        c->valid = 0;
+        c->overflow = 0;
+        c->head = 0;
+    }
+}
+
 // Number of non-sentinel keys in a sorted key array (sentinels sort last).
 __global__ void k_count_valid(const uint32_t* __restrict__ keys, unsigned long long n, unsigned long long* out) {
     unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -407,22 +431,20 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
         nblocks = n_mine;
     }
 
-    unsigned int* head = nullptr;
-    // [0] pair cursor, [1] valid count, [2] tc accepts, [3] tc band pairs, [4] band cursor
-    unsigned long long* counters = nullptr;
-    uint32_t* flags = nullptr;                 // [0] overflow, [1] bounded-wait timeout
-    HJ_TRY(tmp.alloc(&head, 1));
-    HJ_TRY(tmp.alloc(&counters, 8));
-    HJ_TRY(tmp.alloc(&flags, 2));
-    HJ_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
-    HJ_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), st));
-    uint32_t* overflow = flags;
+    // the join's counters and flags: one allocation, reset per batch by one kernel and
+    // read back with one copy
+    JoinCtl* ctl = nullptr;
+    HJ_TRY(tmp.alloc(&ctl, 1));
+    HJ_CUDA(cudaMemsetAsync(ctl, 0, sizeof(JoinCtl), st));
+    unsigned int* head = &ctl->head;
+    uint32_t* overflow = &ctl->overflow;
     PairSink no_band{nullptr, nullptr, nullptr, 0, overflow};
 
     EventPairs kev;   // refine kernel launches of the join proper
+    // head_reset: zero the work-item queue head first (batches reset it with the rest)
     auto run_refine = [&](const HjBlock* blk, uint32_t nb, const PairSink& sink, const PairSink& band,
-                          uint32_t count_only, unsigned long long* bc) -> hj_status {
-        HJ_CUDA(cudaMemsetAsync(head, 0, sizeof(unsigned int), st));
+                          uint32_t count_only, unsigned long long* bc, bool head_reset = true) -> hj_status {
+        if (head_reset) HJ_CUDA(cudaMemsetAsync(head, 0, sizeof(unsigned int), st));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (!count_only) {
             kev.ev.emplace_back(nullptr, nullptr);
@@ -433,14 +455,14 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             HJ_CUDA(cudaEventRecord(e0, st));
         }
         HJ_TRY(tc ? launch_refine_tc(ix, blk, nb, head, sink, band, count_only, bc,
-                                     count_only ? nullptr : counters + 2, flags + 1, st)
+                                     count_only ? nullptr : &ctl->tc_acc, &ctl->timeout, st)
                   : launch_refine_plain(ix, blk, nb, head, sink, count_only, bc, st));
         if (!count_only) HJ_CUDA(cudaEventRecord(e1, st));
         return HJ_OK;
     };
     auto check_timeout = [&]() -> hj_status {
         uint32_t to = 0;
-        HJ_CUDA(cudaMemcpyAsync(&to, flags + 1, 4, cudaMemcpyDeviceToHost, st));
+        HJ_CUDA(cudaMemcpyAsync(&to, &ctl->timeout, 4, cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
         if (to) {
             set_error("hj_join: a bounded device-side wait expired in the tensor-core pipeline");
@@ -614,22 +636,21 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             set_error("hj_join: batch limit %u reached", opts.max_batches);
             return HJ_ERR_OVERFLOW;
         }
-        HJ_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st));
-        HJ_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), st));
-        HJ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(uint32_t), st));
-        PairSink sink{keys, vals, counters, cap, overflow};
-        PairSink band = tc ? PairSink{band_q, band_c, counters + 4, cap, overflow} : no_band;
-        HJ_TRY(run_refine(blocks + b.b0, b.b1 - b.b0, sink, band, 0, nullptr));
-        if (tc) {
-            HJ_TRY(launch_band_recheck(ix, band_q, band_c, counters + 4, cap, sink, b.b1 - b.b0, st));
-            HJ_TRY(check_timeout());
-        }
-        unsigned long long used = 0;
-        uint32_t ovf = 0;
-        HJ_CUDA(cudaMemcpyAsync(&used, counters, 8, cudaMemcpyDeviceToHost, st));
-        HJ_CUDA(cudaMemcpyAsync(&ovf, overflow, 4, cudaMemcpyDeviceToHost, st));
+        k_batch_reset<<<1, 32, 0, st>>>(ctl);
+        HJ_LAUNCHED();
+        PairSink sink{keys, vals, &ctl->cursor, cap, overflow};
+        PairSink band = tc ? PairSink{band_q, band_c, &ctl->band_cursor, cap, overflow} : no_band;
+        HJ_TRY(run_refine(blocks + b.b0, b.b1 - b.b0, sink, band, 0, nullptr, false));
+        if (tc) HJ_TRY(launch_band_recheck(ix, band_q, band_c, &ctl->band_cursor, cap, sink, b.b1 - b.b0, st));
+        JoinCtl hc;
+        HJ_CUDA(cudaMemcpyAsync(&hc, ctl, sizeof(JoinCtl), cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
-        if (ovf) {
+        if (hc.timeout) {
+            set_error("hj_join: a bounded device-side wait expired in the tensor-core pipeline");
+            return HJ_ERR_TIMEOUT;
+        }
+        const unsigned long long used = hc.cursor;
+        if (hc.overflow) {
             if (b.b1 - b.b0 <= 1) {
                 set_error("hj_join: one work item produces more pairs than the result buffer holds (%llu)",
                           (unsigned long long)cap);
@@ -646,9 +667,9 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
         HJ_TRY(radix_sort_u32_u32(keys, vals, keys_tmp, vals_tmp, slots, key_bits, st));
         unsigned long long valid = 0;
         if (slots) {
-            k_count_valid<<<(unsigned)((slots + 255) / 256), 256, 0, st>>>(keys, slots, counters + 1);
+            k_count_valid<<<(unsigned)((slots + 255) / 256), 256, 0, st>>>(keys, slots, &ctl->valid);
             HJ_LAUNCHED();
-            HJ_CUDA(cudaMemcpyAsync(&valid, counters + 1, 8, cudaMemcpyDeviceToHost, st));
+            HJ_CUDA(cudaMemcpyAsync(&valid, &ctl->valid, 8, cudaMemcpyDeviceToHost, st));
             HJ_CUDA(cudaStreamSynchronize(st));
         }
         HJ_TRY(handler.on_batch(n_out, keys, vals, valid, st));
@@ -667,7 +688,7 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     cudaGetLastError();
     if (tc) {
         unsigned long long tcs[2] = {0, 0};
-        HJ_CUDA(cudaMemcpyAsync(tcs, counters + 2, sizeof(tcs), cudaMemcpyDeviceToHost, st));
+        HJ_CUDA(cudaMemcpyAsync(tcs, &ctl->tc_acc, sizeof(tcs), cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
         S.tc_accepts = tcs[0];
         S.band_pairs = tcs[1];

@@ -28,19 +28,20 @@
 // reject.  The result set is therefore identical to the exact path.
 //
 // Kernel shape (one CTA per SM, persistent, 96 + 128 * EPI threads):
-//   warp 0      TMA producer: the query block once per work item, candidate
-//               tiles through a ring of shared-memory stages;
-//   warps 1, 2  MMA issuers, one per TMEM accumulator: per candidate tile,
-//               M = 128 x N = 256 MMAs into 2 accumulators of 256 columns (all
-//               512 TMEM columns), one per half of the query block.  N = 256
-//               matters: a microbenchmark of this pattern issued 128 x 128 x 16
-//               MMAs at 42% of the tensor pipe's rate and 128 x 256 x 16 ones at
-//               98%;
+//   warp 0      TMA producer: the work item's 256 queries once, candidate tiles
+//               through a ring of shared-memory stages;
+//   warps 1, 2  MMA issuers: candidate tile t is computed as M = 128 x N = 256
+//               MMAs into TMEM accumulator t % 2 (2 x 256 columns, all of TMEM)
+//               by issuer 1 + t % 2.  The accumulators form a ring over the
+//               tiles, so the MMAs of tile t + 1 run while the epilogue drains
+//               tile t.  N = 256 matters: a microbenchmark of this pattern
+//               issued 128 x 128 x 16 MMAs at 42% of the tensor pipe's rate and
+//               128 x 256 x 16 ones at 98%;
 //   warps 3..   epilogue, EPI groups of 4 warps (one per TMEM lane quarter),
-//               either all draining both accumulators or split into one set per
-//               accumulator (autotuned): tcgen05.ld, min-reduce, compare,
-//               warp-aggregated emission; an accumulator is released as soon as
-//               its set has read it, so MMA and epilogue overlap.
+//               either all draining every tile or split into one set per
+//               accumulator (every other tile; autotuned): tcgen05.ld,
+//               min-reduce, compare, warp-aggregated emission; an accumulator
+//               is released as soon as its warps have read it.
 // Every wait is bounded; a timeout raises an error flag, drains and returns.
 
 #include <cudaTypedefs.h>
@@ -57,15 +58,18 @@
 namespace hj {
 namespace {
 
-constexpr int kQT = 4;                       // 128-row query loads per work item
+constexpr int kQT = 2;                       // 128-row query loads per work item
 constexpr int kTileRows = 128;               // rows per tile (M for A) and per query load
-constexpr int kQB = kQT * kTileRows;         // queries per work item
-constexpr int kAcc = 2;                      // TMEM accumulators (query halves) per work item
-constexpr int kAccCols = 256;                // N of one MMA: queries per accumulator
+constexpr int kQB = kQT * kTileRows;         // queries per work item (N of every MMA)
+constexpr int kAcc = 2;                      // TMEM accumulators: a ring over the candidate tiles
+constexpr int kAccCols = 256;                // N of one MMA: the work item's queries
 constexpr int kProbeThreads = 192;   // tile probe: TMA warp, MMA warp, 4 epilogue warps
+constexpr int kProbeQT = 4;                  // the tile probe evaluates 512 query rows ...
+constexpr int kProbeQB = kProbeQT * kTileRows;
 constexpr int kMaxStages = 8;
 constexpr uint32_t kKBlockBytes = kTileRows * 64;   // one 32-element K block of a 128-row tile
 constexpr uint32_t kBKBlockBytes = kQB * 64;        // one 32-element K block of the whole query block
+constexpr uint32_t kProbeBKBlockBytes = kProbeQB * 64;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMaxRanges = 256;
 constexpr long long kWaitCycles = 4000000000ll;     // ~2 s at 1.9 GHz
@@ -107,7 +111,7 @@ struct TcShared {
     uint32_t tmem_base;
     uint32_t item;
     uint32_t abort;
-    uint32_t nq, nqt, ntiles, nr, q0;
+    uint32_t nq, ntiles, nr, q0;
     uint32_t max_e, max_n, max_r;          // float bits (non-negative)
     uint32_t qid[kQB];
     uint32_t cidw[16 * 32];                // epilogue warp w, lane l: original id of its current row
@@ -180,12 +184,11 @@ __device__ __forceinline__ float minN(const float (&v)[N]) {
 }
 
 // EPI = epilogue warp groups (4 warps each, one per TMEM lane quarter).  SPLIT:
-// the epilogue warps form one set per accumulator (a warp drains half as many
-// accumulators, each over a whole tile's MMA time) instead of every warp draining
-// both.  Which is faster depends on d: the autotuner times all four shapes.
-// DEFER: one vote per accumulator instead of one per chunk, chunks with a hit
-// read again before the release; it pays where hits are rare (picked from the
-// estimated pair density).
+// the epilogue warps form one set per accumulator, so a warp drains every other
+// tile (with two tiles' MMA time for it) instead of every tile.  Which is faster
+// depends on d: the autotuner times all four shapes.  DEFER: one vote per
+// accumulator instead of one per chunk, chunks with a hit read again before the
+// release; it pays where hits are rare (picked from the estimated pair density).
 template <int EPI, bool SPLIT, bool DEFER>
 __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     k_refine_tc(const __grid_constant__ CUtensorMap tm_cand, const __grid_constant__ CUtensorMap tm_query, TcArgs a) {
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     uint32_t base = tc::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (base & 1023u)) & 1023u);
     const uint32_t tile_bytes = a.nkb * kKBlockBytes;
-    uint8_t* b_tiles = smem;                                   // query block: [K block][512 rows]
+    uint8_t* b_tiles = smem;                                   // query block: [K block][256 rows]
     uint8_t* a_tiles = smem + kQT * tile_bytes;                // a.stages tiles: [K block][128 rows]
     TcShared& S = *reinterpret_cast<TcShared*>(a_tiles + a.stages * tile_bytes);
 
@@ -203,7 +206,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
     if (tid == 0) {
         for (uint32_t s = 0; s < a.stages; ++s) {
             tc::mbar_init(&S.full_a[s], 1);
-            tc::mbar_init(&S.empty_a[s], kAcc);   // one arrival per MMA issuer
+            tc::mbar_init(&S.empty_a[s], 1);   // released by the one issuer of the tile it holds
         }
         for (int j = 0; j < kAcc; ++j) {
             tc::mbar_init(&S.full_acc[j], 1);
@@ -325,21 +328,20 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                 S.ntiles = incl;
                 S.nr = nr;
                 S.nq = nq;
-                S.nqt = (nq + kAccCols - 1) / kAccCols;   // accumulators in use
                 S.q0 = blk.q0;
             }
         }
         __syncthreads();
-        const uint32_t ntiles = S.ntiles, nqt = S.nqt;
+        const uint32_t ntiles = S.ntiles;
         if (ntiles == 0) continue;
 
         if (warp == 0) {
             if (lane == 0) {
                 // ---------------- TMA producer
-                // every row an accumulator's MMA reads is loaded (rows past n are zero-filled)
-                const uint32_t nloads = nqt * (kAccCols / kTileRows);
-                tc::mbar_arrive_expect_tx(&S.bfull, nloads * tile_bytes);
-                for (uint32_t j = 0; j < nloads; ++j)
+                // both query tiles: rows past the item's queries are masked in the epilogue,
+                // rows past n are zero-filled
+                tc::mbar_arrive_expect_tx(&S.bfull, kQT * tile_bytes);
+                for (uint32_t j = 0; j < (uint32_t)kQT; ++j)
                     for (uint32_t kb = 0; kb < a.nkb; ++kb)
                         tc::tma_load_2d(b_tiles + kb * kBKBlockBytes + j * kKBlockBytes, &tm_query, &S.bfull,
                                         (int)(kb * 32), (int)(blk.q0 + j * kTileRows));
@@ -359,44 +361,35 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
             it = __shfl_sync(0xffffffffu, it, 0);
         } else if (warp <= kAcc) {
             if (lane == 0) {
-                // ---------------- MMA issuer of accumulator h (warp 1: h = 0, warp 2: h = 1).
-                // One issuer per accumulator: every barrier wait stalls the issuing thread's
-                // MMA stream for ~160 cycles (measured), and with two issuers the other one
-                // keeps the tensor pipe busy meanwhile.  Both wait for every candidate tile
-                // and both arrive on its stage's empty barrier (count 2), so neither can run
-                // a ring cycle ahead of the other.
+                // ---------------- MMA issuer h (warp 1: h = 0, warp 2: h = 1) of the tiles t with
+                // t % 2 == h, into accumulator h.  Two issuers: every barrier wait stalls the
+                // issuing thread's MMA stream for ~160 cycles (measured), and the other issuer
+                // keeps the tensor pipe busy meanwhile.
                 const uint32_t h = warp - 1;
                 bool ok = tc::mbar_wait(&S.bfull, items_loaded & 1u, abort, a.err, a.wait_cycles);
                 tc::fence_after();
                 const uint32_t ksteps = a.nkb * 2;
                 const uint32_t a_base = tc::smem_u32(a_tiles), b_base = tc::smem_u32(b_tiles);
-                const bool active = h < nqt;
                 for (uint32_t t = 0; ok && t < ntiles; ++t) {
                     const uint32_t s = it % a.stages, use = it / a.stages;
-                    if (!tc::mbar_wait(&S.full_a[s], use & 1u, abort, a.err, a.wait_cycles)) break;
-                    tc::fence_after();
-                    if (active) {
-                        if (acc_use[h] > 0 &&
-                            !tc::mbar_wait(&S.empty_acc[h], (acc_use[h] - 1) & 1u, abort, a.err, a.wait_cycles)) {
-                            ok = false;
-                        } else {
-                            tc::fence_after();
-                            // M = 128 candidates x N = 256 queries per MMA: the shape that keeps
-                            // the tensor pipe busy (N = 128 MMAs issue at well under half its rate)
-                            for (uint32_t ks = 0; ks < ksteps; ++ks) {
-                                const uint32_t kin = (ks & 1u) * 32u;
-                                uint64_t ad = tc::desc_kmajor_sw64(a_base + s * tile_bytes +
-                                                                   (ks >> 1) * kKBlockBytes + kin);
-                                uint64_t bd = tc::desc_kmajor_sw64(b_base + (ks >> 1) * kBKBlockBytes +
-                                                                   h * (kAccCols * 64u) + kin);
-                                tc::mma_f16(tmem + h * kAccCols, ad, bd, a.idesc, ks > 0 ? 1u : 0u);
-                            }
-                            tc::mma_commit(&S.full_acc[h]);
-                            ++acc_use[h];
-                        }
-                    }
-                    tc::mma_commit(&S.empty_a[s]);
                     ++it;
+                    if ((t & 1u) != h) continue;
+                    if (!tc::mbar_wait(&S.full_a[s], use & 1u, abort, a.err, a.wait_cycles)) break;
+                    if (acc_use[h] > 0 &&
+                        !tc::mbar_wait(&S.empty_acc[h], (acc_use[h] - 1) & 1u, abort, a.err, a.wait_cycles))
+                        break;
+                    tc::fence_after();
+                    // M = 128 candidates x N = 256 queries per MMA: the shape that keeps the
+                    // tensor pipe busy (N = 128 MMAs issue at well under half its rate)
+                    for (uint32_t ks = 0; ks < ksteps; ++ks) {
+                        const uint32_t kin = (ks & 1u) * 32u;
+                        uint64_t ad = tc::desc_kmajor_sw64(a_base + s * tile_bytes + (ks >> 1) * kKBlockBytes + kin);
+                        uint64_t bd = tc::desc_kmajor_sw64(b_base + (ks >> 1) * kBKBlockBytes + kin);
+                        tc::mma_f16(tmem + h * kAccCols, ad, bd, a.idesc, ks > 0 ? 1u : 0u);
+                    }
+                    tc::mma_commit(&S.full_acc[h]);
+                    ++acc_use[h];
+                    tc::mma_commit(&S.empty_a[s]);
                 }
             }
             __syncwarp();
@@ -406,13 +399,13 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
             ++items_loaded;
         } else {
             // ---------------- epilogue: warps 3 .. 3 + 4*EPI.  SPLIT: two sets of 2*EPI warps,
-            // one per accumulator, so a warp has a whole tile's MMA time to drain its share
-            // of one accumulator and a slow warp holds back only its own accumulator;
-            // otherwise one set of 4*EPI warps drains both.  TMEM lane quarter = warp % 4;
-            // column group within the set = (index in set) / 4.
+            // one per accumulator (tiles of one parity), so a warp has two tiles' MMA time to
+            // drain its share and a slow warp holds back only its own accumulator; otherwise
+            // one set of 4*EPI warps drains every tile.  TMEM lane quarter = warp % 4; column
+            // group within the set = (index in set) / 4.
             constexpr uint32_t SETW = SPLIT ? 2 * EPI : 4 * EPI;
             const uint32_t ew = warp - 1 - kAcc;
-            const uint32_t hset = ew / SETW;   // SPLIT: the accumulator this warp drains
+            const uint32_t hset = ew / SETW;   // SPLIT: the accumulator (tile parity) this warp drains
             const uint32_t quarter = warp & 3u;
             const uint32_t grp = (ew % SETW) >> 2;
             const uint32_t row = quarter * 32u + lane;
@@ -421,25 +414,29 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
             uint32_t n_acc = 0, n_band = 0;
             bool ok = true;
             // this warp's columns of an accumulator: COLS = 256 / (SETW / 4), read in chunks
-            // of LDW by tcgen05.ld, W chunks per wait ("wave").  EPI 4 leaves 96 registers a
-            // thread: two 32-column chunks per wave when a warp has 64 columns, one when it
-            // has 128.
+            // of LDW by tcgen05.ld, W chunks per wait ("wave").
             constexpr uint32_t COLS = kAccCols / (SETW / 4);
             constexpr uint32_t LDW = EPI == 4 ? 32u : 64u;
             constexpr uint32_t NCH = COLS / LDW;
-            constexpr uint32_t W = (EPI == 4 && !SPLIT) ? 2u : 1u;
+            constexpr uint32_t W = (EPI == 2 || !SPLIT) ? 2u : 1u;
+            static_assert(NCH % W == 0, "whole waves per accumulator");
+            const uint32_t t_first = SPLIT ? hset : 0u, t_step = SPLIT ? 2u : 1u;
+            const uint32_t ncols = min((uint32_t)kAccCols, S.nq);
             TileWalk tw;
-            tw.locate(S, 0);
             // the row's bounds and original id, loaded one tile ahead: a global load on the
             // hit path stalls the warp, and a stalled warp holds back the release of the
             // next accumulator
             float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
             uint32_t cid_next = 0u;
-            if (row < tw.valid) {
-                pc = a.pinfo[tw.start + row];
-                if (!a.count_only) cid_next = a.perm[tw.start + row];
+            if (t_first < ntiles) {
+                tw.locate(S, t_first);
+                if (row < tw.valid) {
+                    pc = a.pinfo[tw.start + row];
+                    if (!a.count_only) cid_next = a.perm[tw.start + row];
+                }
             }
-            for (uint32_t t = 0; ok && t < ntiles; ++t) {
+            for (uint32_t t = t_first; ok && t < ntiles; t += t_step) {
+                const uint32_t j = t & 1u;
                 const uint32_t cpos = tw.start + row;
                 const bool vrow = row < tw.valid;
                 float hi = -INFINITY, lo = -INFINITY;
@@ -449,64 +446,120 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                     hi = __fadd_ru(a.thr, d);
                     lo = __fsub_rd(a.thr, d);
                 }
-                if (t + 1 < ntiles) {
+                if (t + t_step < ntiles) {
                     // the next tile's row bounds, loaded while this tile is processed
-                    tw.locate(S, t + 1);
+                    tw.locate(S, t + t_step);
                 }
                 const uint32_t cid = cid_next;
                 S.cidw[ew * 32 + lane] = cid;   // read by the lanes that write this row's pairs
                 __syncwarp();
-                if (t + 1 < ntiles && row < tw.valid) {
+                if (t + t_step < ntiles && row < tw.valid) {
                     pc = a.pinfo[tw.start + row];
                     if (!a.count_only) cid_next = a.perm[tw.start + row];
                 }
-                const uint32_t j_end = SPLIT ? min(hset + 1, nqt) : nqt;
-                for (uint32_t j = SPLIT ? hset : 0u; j < j_end; ++j) {
-                    if (!tc::mbar_wait(&S.full_acc[j], acc_use[j] & 1u, abort, a.err, a.wait_cycles)) {
-                        ok = false;
-                        break;
+                if (!tc::mbar_wait(&S.full_acc[j], acc_use[j] & 1u, abort, a.err, a.wait_cycles)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after();
+                const uint32_t* cidw = &S.cidw[ew * 32];
+                const uint32_t q0 = S.q0, cpos0 = cpos - lane;
+                if constexpr (DEFER) {
+                    // fast pass: min-reduce every chunk and note, per row, the chunks with a value
+                    // not above the upper band edge; no vote or branch per chunk
+                    uint32_t hitw = 0;
+                    auto load_chunk = [&](float (&v)[LDW], uint32_t c) {
+                        const uint32_t col = grp * COLS + c * LDW;
+                        if constexpr (LDW == 64) tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v);
+                        else tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v);
+                    };
+#pragma unroll 1
+                    for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
+                        float v[W][LDW];
+#pragma unroll
+                        for (uint32_t w = 0; w < W; ++w) load_chunk(v[w], c0 + w);
+                        tc::tmem_ld_wait();
+#pragma unroll
+                        for (uint32_t w = 0; w < W; ++w) hitw |= (uint32_t)not_above(minN<LDW>(v[w]), hi) << (c0 + w);
                     }
-                    tc::fence_after();
-                    const uint32_t ncols = min((uint32_t)kAccCols, nq - j * kAccCols);
-                    if constexpr (DEFER) {
-                        // fast pass: min-reduce every chunk and note, per row, the chunks with a value
-                        // at or below the upper band edge; no vote or branch per chunk
-                        uint32_t hitw = 0;
-                        auto load_chunk = [&](float (&v)[LDW], uint32_t c) {
-                            const uint32_t col = grp * COLS + c * LDW;
-                            if constexpr (LDW == 64) tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v);
-                            else tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v);
-                        };
-    #pragma unroll 1
-                        for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
-                            float v[W][LDW];
-    #pragma unroll
-                            for (uint32_t w = 0; w < W; ++w) load_chunk(v[w], c0 + w);
-                            tc::tmem_ld_wait();
-    #pragma unroll
-                            for (uint32_t w = 0; w < W; ++w) hitw |= (uint32_t)not_above(minN<LDW>(v[w]), hi) << (c0 + w);
+                    // chunks where some row hit are read again (rare: the accumulator is still
+                    // held) and classified pair by pair
+                    uint32_t wave_hits = __reduce_or_sync(0xffffffffu, hitw);
+                    while (wave_hits) {
+                        const uint32_t c = __ffs(wave_hits) - 1;
+                        wave_hits &= wave_hits - 1;
+                        float v[LDW];
+                        load_chunk(v, c);
+                        tc::tmem_ld_wait();
+                        const bool any_hit = (hitw >> c) & 1u;
+                        const uint32_t col0 = grp * COLS + c * LDW;
+#pragma unroll
+                        for (uint32_t h = 0; h < LDW / 32; ++h) {
+                            const uint32_t qcol = col0 + h * 32u;
+                            uint32_t hmask = 0, amask = 0;
+                            if (any_hit) {
+#pragma unroll
+                                for (int i = 0; i < 32; ++i) {
+                                    bool inq = qcol + i < ncols;
+                                    hmask |= (uint32_t)(inq && not_above(v[h * 32 + i], hi)) << i;
+                                    amask |= (uint32_t)(inq && v[h * 32 + i] <= lo) << i;
+                                }
+                            }
+                            const uint32_t bmask = hmask & ~amask;
+                            n_acc += __popc(amask);
+                            n_band += __popc(bmask);
+                            if (a.count_only) continue;
+                            // coalesced output: each lane writes every 32nd pair of the warp's
+                            // hits; the owner lane's row gives the candidate
+                            warp_emit_masks(a.sink, wc_acc, amask, [&](uint32_t owner, uint32_t b) {
+                                return make_uint2(S.qid[qcol + b], cidw[owner]);
+                            });
+                            warp_emit_masks(a.band, wc_band, bmask, [&](uint32_t owner, uint32_t b) {
+                                return make_uint2(q0 + qcol + b, cpos0 + owner);
+                            });
                         }
-                        // chunks where some row hit are read again (rare: the accumulator is still
-                        // held) and classified pair by pair
-                        uint32_t wave_hits = __reduce_or_sync(0xffffffffu, hitw);
-                        while (wave_hits) {
-                            const uint32_t c = __ffs(wave_hits) - 1;
-                            wave_hits &= wave_hits - 1;
-                            float v[LDW];
-                            load_chunk(v, c);
-                            tc::tmem_ld_wait();
-                            const bool any_hit = (hitw >> c) & 1u;
-                            const uint32_t col0 = grp * COLS + c * LDW;
-    #pragma unroll
+                    }
+                    // every column of this warp has been read: release the accumulator
+                    tc::fence_before();
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
+                } else {
+                    // per chunk: min-reduce, vote, and classify at once; the accumulator is
+                    // released as soon as the last wave is in registers
+#pragma unroll 1
+                    for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
+                        float v[W][LDW];
+#pragma unroll
+                        for (uint32_t w = 0; w < W; ++w) {
+                            const uint32_t col = grp * COLS + (c0 + w) * LDW;
+                            if constexpr (LDW == 64) {
+                                tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v[w]);
+                            } else {
+                                tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v[w]);
+                            }
+                        }
+                        tc::tmem_ld_wait();
+                        if (c0 + W >= NCH) {
+                            // all of this warp's columns are in registers: release the accumulator
+                            tc::fence_before();
+                            __syncwarp();
+                            if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
+                        }
+#pragma unroll
+                        for (uint32_t w = 0; w < W; ++w) {
+                            const uint32_t col0 = grp * COLS + (c0 + w) * LDW;
+                            const bool any_hit = not_above(minN<LDW>(v[w]), hi);
+                            if (!__any_sync(0xffffffffu, any_hit)) continue;
+#pragma unroll
                             for (uint32_t h = 0; h < LDW / 32; ++h) {
-                                const uint32_t cbase = col0 + h * 32u;
+                                const uint32_t qcol = col0 + h * 32u;
                                 uint32_t hmask = 0, amask = 0;
                                 if (any_hit) {
-    #pragma unroll
+#pragma unroll
                                     for (int i = 0; i < 32; ++i) {
-                                        bool inq = cbase + i < ncols;
-                                        hmask |= (uint32_t)(inq && not_above(v[h * 32 + i], hi)) << i;
-                                        amask |= (uint32_t)(inq && v[h * 32 + i] <= lo) << i;
+                                        bool inq = qcol + i < ncols;
+                                        hmask |= (uint32_t)(inq && not_above(v[w][h * 32 + i], hi)) << i;
+                                        amask |= (uint32_t)(inq && v[w][h * 32 + i] <= lo) << i;
                                     }
                                 }
                                 const uint32_t bmask = hmask & ~amask;
@@ -515,81 +568,17 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                                 if (a.count_only) continue;
                                 // coalesced output: each lane writes every 32nd pair of the warp's
                                 // hits; the owner lane's row gives the candidate
-                                const uint32_t qcol = j * kAccCols + cbase;
-                                const uint32_t* cidw = &S.cidw[ew * 32];
                                 warp_emit_masks(a.sink, wc_acc, amask, [&](uint32_t owner, uint32_t b) {
                                     return make_uint2(S.qid[qcol + b], cidw[owner]);
                                 });
-                                const uint32_t q0 = S.q0, cpos0 = cpos - lane;
                                 warp_emit_masks(a.band, wc_band, bmask, [&](uint32_t owner, uint32_t b) {
                                     return make_uint2(q0 + qcol + b, cpos0 + owner);
                                 });
                             }
                         }
-                        // every column of this warp has been read: release the accumulator
-                        tc::fence_before();
-                        __syncwarp();
-                        if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
-                    } else {
-                        // per chunk: min-reduce, vote, and classify at once; the accumulator is
-                        // released as soon as the last wave is in registers
-    #pragma unroll 1
-                        for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
-                            float v[W][LDW];
-    #pragma unroll
-                            for (uint32_t w = 0; w < W; ++w) {
-                                const uint32_t col = grp * COLS + (c0 + w) * LDW;
-                                if constexpr (LDW == 64) {
-                                    tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v[w]);
-                                } else {
-                                    tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v[w]);
-                                }
-                            }
-                            tc::tmem_ld_wait();
-                            if (c0 + W >= NCH) {
-                                // all of this warp's columns are in registers: release the accumulator
-                                tc::fence_before();
-                                __syncwarp();
-                                if (lane == 0) tc::mbar_arrive(&S.empty_acc[j]);
-                            }
-    #pragma unroll
-                            for (uint32_t w = 0; w < W; ++w) {
-                                const uint32_t col0 = grp * COLS + (c0 + w) * LDW;
-                                const bool any_hit = not_above(minN<LDW>(v[w]), hi);
-                                if (!__any_sync(0xffffffffu, any_hit)) continue;
-    #pragma unroll
-                                for (uint32_t h = 0; h < LDW / 32; ++h) {
-                                    const uint32_t cbase = col0 + h * 32u;
-                                    uint32_t hmask = 0, amask = 0;
-                                    if (any_hit) {
-    #pragma unroll
-                                        for (int i = 0; i < 32; ++i) {
-                                            bool inq = cbase + i < ncols;
-                                            hmask |= (uint32_t)(inq && not_above(v[w][h * 32 + i], hi)) << i;
-                                            amask |= (uint32_t)(inq && v[w][h * 32 + i] <= lo) << i;
-                                        }
-                                    }
-                                    const uint32_t bmask = hmask & ~amask;
-                                    n_acc += __popc(amask);
-                                    n_band += __popc(bmask);
-                                    if (a.count_only) continue;
-                                    // coalesced output: each lane writes every 32nd pair of the warp's
-                                    // hits; the owner lane's row gives the candidate
-                                    const uint32_t qcol = j * kAccCols + cbase;
-                                    const uint32_t* cidw = &S.cidw[ew * 32];
-                                    warp_emit_masks(a.sink, wc_acc, amask, [&](uint32_t owner, uint32_t b) {
-                                        return make_uint2(S.qid[qcol + b], cidw[owner]);
-                                    });
-                                    const uint32_t q0 = S.q0, cpos0 = cpos - lane;
-                                    warp_emit_masks(a.band, wc_band, bmask, [&](uint32_t owner, uint32_t b) {
-                                        return make_uint2(q0 + qcol + b, cpos0 + owner);
-                                    });
-                                }
-                            }
-                        }
                     }
-                    ++acc_use[j];
                 }
+                ++acc_use[j];
             }
             unsigned long long w_acc = n_acc, w_band = n_band;
             for (int o = 16; o > 0; o >>= 1) {
@@ -773,7 +762,7 @@ __global__ void __launch_bounds__(kProbeThreads, 1)
     uint8_t* smem = smem_raw + ((1024u - (base & 1023u)) & 1023u);
     const uint32_t tile_bytes = nkb * kKBlockBytes;
     uint8_t* b_tiles = smem;
-    uint8_t* a_tile = smem + kQT * tile_bytes;
+    uint8_t* a_tile = smem + kProbeQT * tile_bytes;
     uint64_t* bars = reinterpret_cast<uint64_t*>(a_tile + tile_bytes);   // [0] loads, [1] mma
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
     uint32_t* abortp = tslot + 1;
@@ -793,11 +782,11 @@ __global__ void __launch_bounds__(kProbeThreads, 1)
     tc::fence_after();
     const uint32_t tmem = *tslot;
     if (tid == 0) {
-        tc::mbar_arrive_expect_tx(&bars[0], (kQT + 1) * tile_bytes);
+        tc::mbar_arrive_expect_tx(&bars[0], (kProbeQT + 1) * tile_bytes);
         for (uint32_t kb = 0; kb < nkb; ++kb) {
             tc::tma_load_2d(a_tile + kb * kKBlockBytes, &tm_cand, &bars[0], (int)(kb * 32), (int)a0);
-            for (uint32_t j = 0; j < kQT; ++j)
-                tc::tma_load_2d(b_tiles + kb * kBKBlockBytes + j * kKBlockBytes, &tm_query, &bars[0], (int)(kb * 32),
+            for (uint32_t j = 0; j < kProbeQT; ++j)
+                tc::tma_load_2d(b_tiles + kb * kProbeBKBlockBytes + j * kKBlockBytes, &tm_query, &bars[0], (int)(kb * 32),
                                 (int)(b0 + j * kTileRows));
         }
     }
@@ -812,7 +801,7 @@ __global__ void __launch_bounds__(kProbeThreads, 1)
                     const uint32_t kin = (ks & 1u) * 32u;
                     tc::mma_f16(tmem + j * kAccCols,
                                 tc::desc_kmajor_sw64(tc::smem_u32(a_tile) + (ks >> 1) * kKBlockBytes + kin),
-                                tc::desc_kmajor_sw64(tc::smem_u32(b_tiles) + (ks >> 1) * kBKBlockBytes +
+                                tc::desc_kmajor_sw64(tc::smem_u32(b_tiles) + (ks >> 1) * kProbeBKBlockBytes +
                                                      j * (kAccCols * 64u) + kin),
                                 idesc, ks > 0 ? 1u : 0u);
                 }
@@ -825,12 +814,12 @@ __global__ void __launch_bounds__(kProbeThreads, 1)
         bool ok = tc::mbar_wait(&bars[1], 0, abortp, err, wait_cycles);
         tc::fence_after();
         if (ok) {
-            for (uint32_t col = 0; col < (uint32_t)kQB; col += 32) {
+            for (uint32_t col = 0; col < (uint32_t)kProbeQB; col += 32) {
                 float v[32];
                 tc::tmem_ld_32x32(tmem + ((quarter * 32u) << 16) + col, v);
                 tc::tmem_ld_wait();
 #pragma unroll
-                for (int i = 0; i < 32; ++i) out[(size_t)(quarter * 32 + lane) * kQB + col + i] = v[i];
+                for (int i = 0; i < 32; ++i) out[(size_t)(quarter * 32 + lane) * kProbeQB + col + i] = v[i];
             }
         }
     }
@@ -1153,7 +1142,7 @@ static hj_status run_tile_probe(hj_index* ix, int kind, uint32_t a0, uint32_t b0
     HJ_TRY(tc_prepare(ix, kind, st));
     TcState* s = tc_state(ix);
     const uint32_t nkb = ix->tc_kpad / 32;
-    size_t smem = 1024 + (size_t)(kQT + 1) * nkb * kKBlockBytes + 64;
+    size_t smem = 1024 + (size_t)(kProbeQT + 1) * nkb * kKBlockBytes + 64;
     smem = std::max<size_t>(smem, 116 * 1024);
     HJ_TRY(ensure_smem(k_tc_tile_probe, smem));
     Scratch tmp(st);
@@ -1168,7 +1157,7 @@ static hj_status run_tile_probe(hj_index* ix, int kind, uint32_t a0, uint32_t b0
     HJ_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
     if (h_query_rows)
         HJ_CUDA(cudaMemcpyAsync(h_query_rows, (const uint16_t*)ix->tc_a + (size_t)b0 * ix->tc_kpad,
-                                (size_t)std::min<uint32_t>(kQB, ix->n - b0) * ix->tc_kpad * 2, cudaMemcpyDeviceToHost, st));
+                                (size_t)std::min<uint32_t>(kProbeQB, ix->n - b0) * ix->tc_kpad * 2, cudaMemcpyDeviceToHost, st));
     if (h_cand_rows)
         HJ_CUDA(cudaMemcpyAsync(h_cand_rows, (const uint16_t*)ix->tc_b + (size_t)a0 * ix->tc_kpad,
                                 (size_t)std::min<uint32_t>(kTileRows, ix->n - a0) * ix->tc_kpad * 2,
@@ -1195,7 +1184,7 @@ extern "C" hj_status hj_probe_tc_wait_timeout(hj_index* ix, int kind, uint64_t w
     cudaStream_t st = as_stream(stream);
     Scratch tmp(st);
     float* out = nullptr;
-    HJ_TRY(tmp.alloc(&out, (size_t)kTileRows * kQB));
+    HJ_TRY(tmp.alloc(&out, (size_t)kTileRows * kProbeQB));
     return run_tile_probe(ix, kind, 0, 0, out, 1u, (long long)wait_cycles, nullptr, nullptr, st);
 }
 

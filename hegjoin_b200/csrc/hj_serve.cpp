@@ -24,9 +24,14 @@
 #include <vector>
 
 #include "hegjoin_b200.h"
+#include "hj_workspace.h"
 
 namespace hj {
 void result_set_stream(hj_result* r, cudaStream_t s);   // hj_join.cu
+}
+
+namespace {
+constexpr size_t kWorkspaceBytes = 256ull << 20;   // per worker
 }
 
 namespace {
@@ -85,6 +90,16 @@ void worker_main(hj_server* S) {
     cudaSetDevice(S->device);
     cudaStream_t st;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    // the worker's device workspace: the temporaries of its requests' index builds and
+    // joins come from it, so a small request makes no allocator calls for them
+    hj::Workspace ws;
+    ws.stream = st;
+    if (cudaMallocAsync((void**)&ws.base, kWorkspaceBytes, st) == cudaSuccess) {
+        ws.cap = kWorkspaceBytes;
+        hj::set_current_workspace(&ws);
+    } else {
+        cudaGetLastError();   // no workspace: every temporary comes from the pool
+    }
     for (;;) {
         Req* r = nullptr;
         {
@@ -142,6 +157,9 @@ void worker_main(hj_server* S) {
         S->cv_done.notify_all();
         S->cv_work.notify_all();
     }
+    hj::set_current_workspace(nullptr);
+    if (ws.base) cudaFreeAsync(ws.base, st);
+    cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
 }
 

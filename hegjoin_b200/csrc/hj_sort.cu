@@ -66,7 +66,9 @@ __global__ void k_scan_sums(Out* sums, uint64_t m) {
     }
 }
 
-// Block-wide exclusive scan of one tile plus the tile's offset.
+// Block-wide exclusive scan of one tile plus the tile's offset (none when
+// offsets is null: a scan of a single tile).  Every element is read and
+// written by the same thread, so the scan may run in place.
 template <typename In, typename Out>
 __global__ void k_scan_tiles(const In* in, Out* out, uint64_t n, const Out* __restrict__ offsets) {
     __shared__ Out warp_tot[kScanBlock / 32];
@@ -97,7 +99,7 @@ __global__ void k_scan_tiles(const In* in, Out* out, uint64_t n, const Out* __re
         warp_tot[threadIdx.x] = wi - w;
     }
     __syncthreads();
-    Out run = offsets[blockIdx.x] + warp_tot[threadIdx.x >> 5] + incl - acc;
+    Out run = (offsets ? offsets[blockIdx.x] : Out(0)) + warp_tot[threadIdx.x >> 5] + incl - acc;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
         uint64_t idx = base + i;
@@ -110,6 +112,13 @@ template <typename In, typename Out>
 hj_status exclusive_scan(const In* in, Out* out, uint64_t n, cudaStream_t st) {
     if (n == 0) return HJ_OK;
     uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles == 1) {
+        // one tile: a single launch and no partial sums (small scans are most of a
+        // small join's, including every pass of the radix sorts of small inputs)
+        k_scan_tiles<In, Out><<<1, kScanBlock, 0, st>>>(in, out, n, nullptr);
+        HJ_LAUNCHED();
+        return HJ_OK;
+    }
     Scratch tmp(st);
     Out* sums = nullptr;
     HJ_TRY(tmp.alloc(&sums, tiles));
