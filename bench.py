@@ -291,9 +291,20 @@ def serving_run(n_requests: int, max_n: int, min_n: int = 1000, workers: int = 8
         reqs.append((db, min(d, 6), quick_eps(db, target, dev, i), target))
     total_pts = sum(r[0].shape[0] for r in reqs)
 
+    # one server per (workers, refine), created and warmed before any timed run: the
+    # measurements are of a running service, not of its start-up (worker threads,
+    # streams, workspaces)
+    servers = {}
+
+    def server(nworkers, refine_kind):
+        key = (nworkers, refine_kind)
+        if key not in servers:
+            servers[key] = hj.Server(workers=nworkers, hbm_budget=int(hbm_budget_gb * (1 << 30)), refine=refine_kind)
+        return servers[key]
+
     def run(nworkers, arrivals, todo=None, refine_kind=None):
         todo = reqs[:len(arrivals)] if todo is None else todo
-        srv = hj.Server(workers=nworkers, hbm_budget=int(hbm_budget_gb * (1 << 30)), refine=refine_kind or refine)
+        srv = server(nworkers, refine_kind or refine)
         tickets = [None] * len(todo)
         t0 = time.perf_counter()
 
@@ -316,18 +327,20 @@ def serving_run(n_requests: int, max_n: int, min_n: int = 1000, workers: int = 8
             infos.append(info)
         th.join()
         span = max(x.t_done for x in infos) - min(x.t_submit for x in infos)
-        srv.close()
         return {"pairs": int(pairs), "seconds": span, "pairs_per_s": pairs / span,
                 "requests_per_s": len(todo) / span,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "mean_ms": float(np.mean(lat) * 1e3)}
 
-    # warm-up: one request of every dimension class (tile-shape tuning, memory pools)
+    # warm-up of every server used below: one request of every dimension class per worker
+    # (tile-shape tuning, memory pools, each worker's first allocations)
     first = {}
     for r in reqs:
         first.setdefault(r[0].shape[1], r)
-    run(1, np.zeros(len(first)), list(first.values()))
-    run(1, np.zeros(len(first)), list(first.values()), refine_kind="exact")
+    warm = list(first.values())
+    run(1, np.zeros(len(warm)), warm)
+    run(1, np.zeros(len(warm)), warm, refine_kind="exact")
+    run(workers, np.zeros(len(warm) * workers), warm * workers)
     serial = run(1, np.zeros(len(reqs)))
     serial_plain = run(1, np.zeros(len(reqs)), refine_kind="exact") if with_plain else None
     capacity = run(workers, np.zeros(len(reqs)))
@@ -335,6 +348,8 @@ def serving_run(n_requests: int, max_n: int, min_n: int = 1000, workers: int = 8
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
     served = run(workers, arrivals)
     served["offered_seconds"] = float(arrivals[-1])
+    for srv in servers.values():
+        srv.close()
     out = {"requests": len(reqs), "points_total": int(total_pts), "n_range": [min_n, max_n],
            "d_choices": [2, 6, 18, 32, 90], "k": "min(d, 6)", "target_neighbours": "U[4, 128]",
            "arrivals": "Poisson", "offered_rate_req_per_s": rate,
@@ -449,6 +464,51 @@ def compare_bench(args, wl):
 
 
 # ---------------------------------------------------------------------------------------------
+# the grid-index build and workload order alone: --index
+def index_bench(args, wl):
+    """GridIndex (cell ids, radix sort, cell table, gathered points, cell hash) plus
+    sort_by_workload, timed with CUDA events, against their algorithmic bytes:
+    build n*d*s read + n*d*s written in cell order + 12*n (u64 key + u32 id) +
+    16*nC; workload order nC*(3^(k-1)*4 + 8) (one row lookup per stencil row)."""
+    import torch
+    import hegjoin_b200 as hj
+    dev = torch.device("cuda", 0)
+    np_db = wl.generate()
+    db = torch.from_numpy(np_db).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(512 * 1000 * 1000 // 4, dtype=torch.float32, device=dev)
+    s = 4 if wl.dtype == "f32" else 8
+    t_build, t_sort = [], []
+    nc = 0
+    for it in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        ix = hj.GridIndex(db, wl.k, wl.eps)
+        e[1].record(stream)
+        ix.sort_by_workload()
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        nc = ix.info().n_nonempty_cells
+        ix.close()
+        if it >= args.warmup:
+            t_build.append(e[0].elapsed_time(e[1]))
+            t_sort.append(e[1].elapsed_time(e[2]))
+    pk, pk_kind = peaks()
+    b_build = 2.0 * wl.n * wl.d * s + 12.0 * wl.n + 16.0 * nc
+    b_sort = nc * (3 ** (wl.k - 1) * 4.0 + 8.0)
+    mb, ms_ = statistics.mean(t_build), statistics.mean(t_sort)
+    print(json.dumps({"metric": "grid-index build and workload order (achieved HBM GB/s)", "workload": wl.name,
+                      "n": wl.n, "d": wl.d, "k": wl.k, "non_empty_cells": nc, "steps": args.steps,
+                      "timing": "CUDA events on the launching stream; a 512 MB buffer written before each step",
+                      "build": {"ms": mb, "algorithmic_bytes": b_build, "achieved_gbs": b_build / mb / 1e6,
+                                "frac": b_build / mb / 1e6 / pk["hbm_gbs"]},
+                      "workload_order": {"ms": ms_, "algorithmic_bytes": b_sort, "achieved_gbs": b_sort / ms_ / 1e6,
+                                         "frac": b_sort / ms_ / 1e6 / pk["hbm_gbs"]},
+                      "peak": {"hbm_gbs": pk["hbm_gbs"], "kind": f"{pk_kind} copy bandwidth"}}), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
 # dataset ingest at the skewed 6-D configuration's size: --ingest
 def ingest_bench(args, wl):
     """The reference's text importer (import_dataset.cpp:10-40, restated in the oracle
@@ -516,6 +576,8 @@ def main():
     ap.add_argument("--compare", action="store_true", help="time the exact refine against the tensor-core filter")
     ap.add_argument("--tc-kind", default="auto", choices=["auto", "tc_f16", "tc_bf16"])
     ap.add_argument("--ingest", action="store_true", help="time the text importer against the reference's")
+    ap.add_argument("--index", action="store_true", help="time the index build and workload order alone")
+    ap.add_argument("--peaks", action="store_true", help="measure this library's pipe peaks (hj_measure_peaks)")
     args = ap.parse_args()
     if args.serve:
         serve_bench(args)
@@ -534,6 +596,15 @@ def main():
         return
     if args.ingest:
         ingest_bench(args, wl)
+        return
+    if args.index:
+        index_bench(args, wl)
+        return
+    if args.peaks:
+        import hegjoin_b200 as hj
+        with ClockSampler(0) as clk:
+            pk = hj.measure_peaks()
+        print(json.dumps({"metric": "measured pipe peaks (TFLOP/s)", **pk, "clocks": clk.summary()}), flush=True)
         return
 
     import torch
@@ -731,6 +802,10 @@ def main():
         extras["serving"]["clocks"] = clk5.summary()
         extras["serving"]["stream"] = ("96 requests, n log-uniform in [1e3, 1e5] (the full request stream of "
                                        "4,096 requests up to 1e6 points runs with --serve)")
+        with ClockSampler(local) as clk6:
+            extras["serving_small"] = serving_run(256, 20_000, workers=8, load=5.0, seed=args.serve_seed + 1)
+        extras["serving_small"]["clocks"] = clk6.summary()
+        extras["serving_small"]["stream"] = "256 small requests, n log-uniform in [1e3, 2e4]"
 
     if rank == 0:
         line = {

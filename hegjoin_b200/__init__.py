@@ -83,6 +83,15 @@ class BatchView(ctypes.Structure):
 BATCH_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(BatchView), ctypes.c_void_p, ctypes.c_void_p)
 
 
+class Peaks(ctypes.Structure):
+    _fields_ = [("fp32_fma_tflops", ctypes.c_double), ("fp32x2_fma_tflops", ctypes.c_double),
+                ("fp64_fma_tflops", ctypes.c_double), ("f16_mma_tflops", ctypes.c_double),
+                ("bf16_mma_tflops", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class ServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_uint64), ("workers", ctypes.c_uint32), ("refine", ctypes.c_int)]
 
@@ -127,6 +136,7 @@ def _load() -> ctypes.CDLL:
         "hj_shard_plan_lpt": (I, [P, U32, U32, U32, P, P]),
         "hj_join_stream": (I, [P, P, BATCH_SINK, P, P, P, P, P, P]),
         "hj_debug_fail_alloc": (None, [U64]),
+        "hj_measure_peaks": (I, [P, P]),
         "hj_debug_pool_used": (I, [P]),
         "hj_import_text": (I, [ctypes.c_char_p, U32, I, P, P]),
         "hj_import_binary": (I, [ctypes.c_char_p, U32, I, P, P]),
@@ -392,6 +402,13 @@ def shard_plan_lpt(costs, shard_count: int, shard_index: int) -> np.ndarray:
     m = ctypes.c_uint32()
     check(lib.hj_shard_plan_lpt(c.ctypes.data, len(c), shard_count, shard_index, items.ctypes.data, ctypes.byref(m)))
     return items[:m.value]
+
+
+def measure_peaks(stream=None) -> dict:
+    """This library's own measured pipe peaks in TFLOP/s (hj_measure_peaks)."""
+    p = Peaks()
+    check(lib.hj_measure_peaks(ctypes.byref(p), _stream_ptr(stream)))
+    return p.as_dict()
 
 
 def debug_fail_alloc(nth: int) -> None:

@@ -311,6 +311,23 @@ void hj_debug_fail_alloc(uint64_t nth);
  * every stream-ordered allocation of the library comes from). */
 hj_status hj_debug_pool_used(uint64_t* bytes);
 
+/* ---- measured peaks (roofline denominators) ---------------------------------- */
+/* Throughput of the pipes the refine kernels run on, measured by this library's
+ * own kernels with CUDA events on `stream` (each runs over every SM for a few to
+ * tens of ms): FP32 FMA chains (scalar and the packed f32x2 form the exact refine
+ * uses), FP64 FMA chains, and tensor-core kind::f16 MMAs of M = 128, N = 256,
+ * K = 16 issued back to back by two threads per SM into TMEM (the filter's issue
+ * pattern), with FP16 and with BF16 inputs.  A flop is one multiply or one add.
+ * No reference counterpart.  Synchronises `stream`. */
+typedef struct {
+    double fp32_fma_tflops;
+    double fp32x2_fma_tflops;
+    double fp64_fma_tflops;
+    double f16_mma_tflops;
+    double bf16_mma_tflops;
+} hj_peaks;
+hj_status hj_measure_peaks(hj_peaks* out, void* stream);
+
 /* ---- probes --------------------------------------------------------------- */
 /* Evaluates the reference's squared-distance expression (kernel.cu:350-353)
  * as nvcc compiles it by default, for n pairs of d-dimensional rows; writes
