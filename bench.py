@@ -789,6 +789,14 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(np_db, wl, seconds_target=20.0)
 
+    # this library's own measured pipe peaks: a second denominator beside the driver's
+    own = None
+    if ws == 1 and not args.no_extras:
+        own = hj.measure_peaks()
+        if tc:
+            roof["own_mma_peak_tflops"] = own["f16_mma_tflops"]
+            roof["frac_of_own_mma_peak"] = roof["achieved"] / own["f16_mma_tflops"]
+
     # the north-star comparisons, each with its own clock record (single GPU only)
     extras = {}
     if ws == 1 and not args.no_extras and wl.name == "c2_18d":
@@ -797,6 +805,16 @@ def main():
         with ClockSampler(local) as clk3:
             extras["tc_vs_plain"] = tc_vs_plain(wlmod.WORKLOADS["c3_90d"], args.extra_steps, 1)
         extras["tc_vs_plain"]["clocks"] = clk3.summary()
+        t3 = extras["tc_vs_plain"]
+        c3 = wlmod.WORKLOADS["c3_90d"]
+        cand3 = t3["plain_fp32"]["candidates"]
+        # plain FP32: 3 d flops per candidate (sub, multiply, add) on the FP32 pipe; the filter:
+        # 2 d per candidate on the tensor pipe (the MMA itself does 2 Kpad)
+        for arm, flops_per, peak_key in (("plain_fp32", 3.0 * c3.d, "fp32x2_fma_tflops"),
+                                          ("tc_filter", 2.0 * c3.d, "f16_mma_tflops")):
+            ach = flops_per * cand3 / (t3[arm]["refine_kernel_ms"] / 1e3) / 1e12
+            t3[arm]["roofline"] = {"achieved_tflops": ach, "own_peak_tflops": own[peak_key],
+                                   "frac_of_own_peak": ach / own[peak_key], "peak": peak_key}
         with ClockSampler(local) as clk5:
             extras["serving"] = serving_run(96, 100_000, workers=8, load=5.0, seed=args.serve_seed)
         extras["serving"]["clocks"] = clk5.summary()
@@ -822,7 +840,7 @@ def main():
                               "kept on the device (per-batch neighbour ids + neighbour table)",
                     "parallelism": f"query-block shards x{ws}" if ws > 1 else "single GPU"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk.summary(), **extras,
+            "clocks": clk.summary(), "peaks_own": own, **extras,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
