@@ -59,7 +59,7 @@ class JoinOpts(ctypes.Structure):
     _fields_ = [("refine", ctypes.c_int), ("result_capacity", ctypes.c_uint64), ("sample_rate", ctypes.c_double),
                 ("mem_fraction", ctypes.c_double), ("query_block", ctypes.c_uint32), ("max_batches", ctypes.c_uint32),
                 ("use_graphs", ctypes.c_uint32), ("keep_keys", ctypes.c_uint32), ("shard_count", ctypes.c_uint32),
-                ("shard_index", ctypes.c_uint32)]
+                ("shard_index", ctypes.c_uint32), ("device_bytes_cap", ctypes.c_uint64)]
 
 
 class JoinStats(ctypes.Structure):
@@ -68,7 +68,7 @@ class JoinStats(ctypes.Structure):
                 ("filter_delta", ctypes.c_double), ("ms_estimate", ctypes.c_float), ("ms_refine", ctypes.c_float),
                 ("ms_group", ctypes.c_float), ("ms_total", ctypes.c_float), ("ms_refine_kernel", ctypes.c_float),
                 ("refine_launches", ctypes.c_uint32), ("refine_used", ctypes.c_uint32),
-                ("kernel_launches", ctypes.c_uint32), ("ms_setup", ctypes.c_float)]
+                ("kernel_launches", ctypes.c_uint32), ("ms_setup", ctypes.c_float), ("bytes_wanted", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -98,7 +98,8 @@ class ServerOpts(ctypes.Structure):
 
 class ServeInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
-                ("t_done", ctypes.c_double), ("stats", JoinStats)]
+                ("t_done", ctypes.c_double), ("stats", JoinStats), ("reserved_bytes", ctypes.c_uint64),
+                ("regrants", ctypes.c_uint32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -138,6 +139,7 @@ def _load() -> ctypes.CDLL:
         "hj_debug_fail_alloc": (None, [U64]),
         "hj_measure_peaks": (I, [P, P]),
         "hj_debug_pool_used": (I, [P]),
+        "hj_debug_pool_peak": (I, [P, I]),
         "hj_import_text": (I, [ctypes.c_char_p, U32, I, P, P]),
         "hj_import_binary": (I, [ctypes.c_char_p, U32, I, P, P]),
         "hj_write_binary": (I, [ctypes.c_char_p, P, U64, U32, I]),
@@ -147,6 +149,7 @@ def _load() -> ctypes.CDLL:
         "hj_server_submit": (I, [P, P, U32, U32, U32, I, D, P]),
         "hj_server_wait": (I, [P, U64, D, P, P]),
         "hj_server_destroy": (I, [P]),
+        "hj_server_usage": (I, [P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -333,7 +336,7 @@ class JoinResult:
 
 
 def join_opts(refine="auto", result_capacity=0, sample_rate=0.0, mem_fraction=0.0, max_batches=0,
-              use_graphs=False, keep_keys=False, shard_count=0, shard_index=0) -> JoinOpts:
+              use_graphs=False, keep_keys=False, shard_count=0, shard_index=0, device_bytes_cap=0) -> JoinOpts:
     o = JoinOpts()
     lib.hj_join_opts_default(ctypes.byref(o))
     o.refine = REFINE_NAMES[refine] if isinstance(refine, str) else int(refine)
@@ -347,6 +350,7 @@ def join_opts(refine="auto", result_capacity=0, sample_rate=0.0, mem_fraction=0.
     o.keep_keys = int(bool(keep_keys))
     o.shard_count = int(shard_count)
     o.shard_index = int(shard_index)
+    o.device_bytes_cap = int(device_bytes_cap)
     return o
 
 
@@ -355,7 +359,11 @@ def join(index: GridIndex, stream=None, **kw) -> JoinResult:
     o = join_opts(**kw)
     st = JoinStats()
     h = ctypes.c_void_p()
-    check(lib.hj_join(index.handle, ctypes.byref(o), _stream_ptr(stream), ctypes.byref(h), ctypes.byref(st)))
+    status = lib.hj_join(index.handle, ctypes.byref(o), _stream_ptr(stream), ctypes.byref(h), ctypes.byref(st))
+    if status != HJ_OK:
+        err = HJError(status, last_error())
+        err.stats = st          # what the join knew (bytes_wanted when its cap refused it)
+        raise err
     return JoinResult(h, st, index.info().n, index.db.device)
 
 
@@ -419,6 +427,13 @@ def debug_fail_alloc(nth: int) -> None:
 def debug_pool_used() -> int:
     b = ctypes.c_uint64()
     check(lib.hj_debug_pool_used(ctypes.byref(b)))
+    return int(b.value)
+
+
+def debug_pool_peak(reset: bool = False) -> int:
+    """Most bytes the library's memory pool held since the last reset."""
+    b = ctypes.c_uint64()
+    check(lib.hj_debug_pool_peak(ctypes.byref(b), int(bool(reset))))
     return int(b.value)
 
 
@@ -588,6 +603,12 @@ class Server:
             import torch
             res = JoinResult(h, info.stats, db.shape[0], torch.device("cuda"))
         return res, info
+
+    def usage(self) -> tuple:
+        """(bytes held against the budget now, the most ever held)."""
+        cur, peak = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib.hj_server_usage(self._h, ctypes.byref(cur), ctypes.byref(peak)))
+        return cur.value, peak.value
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

@@ -514,6 +514,21 @@ hj_status hj_debug_pool_used(uint64_t* bytes) {
     *bytes = (uint64_t)used;
     return HJ_OK;
 }
+hj_status hj_debug_pool_peak(uint64_t* bytes, int reset) {
+    if (!bytes) { set_error("hj_debug_pool_peak: null argument"); return HJ_ERR_INVALID; }
+    int dev = 0;
+    cudaMemPool_t pool;
+    HJ_CUDA(cudaGetDevice(&dev));
+    HJ_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    unsigned long long high = 0;
+    HJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &high));
+    *bytes = (uint64_t)high;
+    if (reset) {
+        unsigned long long zero = 0;   // resets the high-water mark to the current use
+        HJ_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+    }
+    return HJ_OK;
+}
 const char* hj_version(void) { return "hegjoin_b200 0.1 (sm_100a)"; }
 uint64_t hj_kernel_launch_count(void) { return hj::launch_count(); }
 

@@ -353,9 +353,11 @@ struct BatchHandler {
 // work items (optionally this rank's share), estimator, result-buffer sizing,
 // batches with overflow split-and-retry, grouping by query id.  Every device
 // temporary lives in `tmp` and is freed on every return path.
-// kept_bytes_per_pair: device bytes the handler keeps per result pair (left free).
+// kept_bytes_per_pair: device bytes the handler keeps per result pair (left free);
+// fixed_kept_bytes: what the caller already holds for the result (counted against
+// opts.device_bytes_cap).
 hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, BatchHandler& handler,
-                    double kept_bytes_per_pair, hj_join_stats* stats) {
+                    double kept_bytes_per_pair, uint64_t fixed_kept_bytes, hj_join_stats* stats) {
     auto t_start = std::chrono::steady_clock::now();
     hj_join_opts opts;
     if (opts_in) opts = *opts_in; else hj_join_opts_default(&opts);
@@ -568,8 +570,23 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     const uint64_t want = (uint64_t)(total_est * 2.0) + chunk_slack + 4096;
     uint64_t cap = opts.result_capacity ? opts.result_capacity + chunk_slack : want;
     if (cap < chunk_slack * 2) cap = chunk_slack * 2;
-    // the device-wide free-memory query (a driver call) only when the buffers are large
     const double result_bytes = kept_bytes_per_pair * total_est * 1.1;   // what the handler keeps
+    S.bytes_wanted = (uint64_t)((double)cap * bytes_per_slot + result_bytes) + fixed_kept_bytes;
+    // the caller's cap (a serving loop's reservation): smaller buffers mean more batches; a
+    // join that cannot fit even two warp chunks per emitting warp beside its results is refused
+    const uint64_t cap_bytes = opts.device_bytes_cap;
+    if (cap_bytes) {
+        const double room = (double)cap_bytes - (double)fixed_kept_bytes - result_bytes;
+        const uint64_t fit = room > 0 ? (uint64_t)(room / bytes_per_slot) : 0;
+        cap = std::min(cap, fit);
+        if (cap < chunk_slack * 2) {
+            set_error("hj_join: the join needs about %llu device bytes, more than its cap of %llu",
+                      (unsigned long long)S.bytes_wanted, (unsigned long long)cap_bytes);
+            if (stats) *stats = S;
+            return HJ_ERR_OOM;
+        }
+    }
+    // the device-wide free-memory query (a driver call) only when the buffers are large
     auto max_cap_from_free = [&](uint64_t* out) -> hj_status {
         size_t free_b = 0, total_b = 0;
         HJ_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -628,6 +645,7 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     auto t_ref = std::chrono::steady_clock::now();
     float ms_group = 0;
     uint64_t total = 0;
+    double kept = (double)fixed_kept_bytes + (double)cap * bytes_per_slot;   // against the cap
     uint32_t n_out = 0;
     while (!batches.empty()) {
         Batch b = batches.back();
@@ -672,6 +690,21 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             HJ_CUDA(cudaMemcpyAsync(&valid, &ctl->valid, 8, cudaMemcpyDeviceToHost, st));
             HJ_CUDA(cudaStreamSynchronize(st));
         }
+        if (cap_bytes && kept + kept_bytes_per_pair * (double)valid > (double)cap_bytes) {
+            // the estimate was low: refuse before the results pass the cap, asking for the
+            // results so far extrapolated over the remaining work items (heaviest first, so
+            // this errs high)
+            const double slab_b = (double)cap * bytes_per_slot;
+            const double so_far = kept - (double)fixed_kept_bytes - slab_b + kept_bytes_per_pair * (double)valid;
+            const double frac = (double)std::max<uint32_t>(1, b.b1) / nblocks;
+            S.bytes_wanted = std::max<uint64_t>(
+                S.bytes_wanted, (uint64_t)((double)fixed_kept_bytes + slab_b + 1.1 * so_far / frac));
+            set_error("hj_join: the results outgrow the cap of %llu device bytes",
+                      (unsigned long long)cap_bytes);
+            if (stats) *stats = S;
+            return HJ_ERR_OOM;
+        }
+        kept += kept_bytes_per_pair * (double)valid;
         HJ_TRY(handler.on_batch(n_out, keys, vals, valid, st));
         ++n_out;
         total += valid;
@@ -842,7 +875,7 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts, void* stream, hj_resul
     const bool keep_keys = opts && opts->keep_keys;
     RetainHandler h(res, keep_keys);
     hj_join_stats S{};
-    if (s == HJ_OK) s = join_impl(ix, opts, st, h, keep_keys ? 8.0 : 4.0, &S);
+    if (s == HJ_OK) s = join_impl(ix, opts, st, h, keep_keys ? 8.0 : 4.0, (uint64_t)ix->n * sizeof(hj_nt_entry), &S);
     if (s == HJ_OK && !res->vals.empty()) {
         s = dalloc(&res->d_batch_vals, res->vals.size(), st);
         if (s == HJ_OK)
@@ -850,11 +883,11 @@ hj_status hj_join(hj_index* ix, const hj_join_opts* opts, void* stream, hj_resul
                                             cudaMemcpyHostToDevice, st), "batch pointer table");
     }
     if (s == HJ_OK) s = cuda_status(cudaStreamSynchronize(st), "hj_join");
+    if (stats) *stats = S;   // on an error: what was known (bytes_wanted when the cap refused)
     if (s != HJ_OK) {
         hj_result_destroy(res);
         return s;
     }
-    if (stats) *stats = S;
     *out = res;
     return HJ_OK;
 }
@@ -873,7 +906,7 @@ hj_status hj_join_stream(hj_index* ix, const hj_join_opts* opts, hj_batch_sink s
         HJ_CUDA(cudaMemsetAsync(d_xor, 0, (size_t)ix->n * 8, st));
     }
     StreamHandler h(sink, user, d_count, d_sum, d_xor);
-    HJ_TRY(join_impl(ix, opts, st, h, 0.0, stats));
+    HJ_TRY(join_impl(ix, opts, st, h, 0.0, 0, stats));
     HJ_CUDA(cudaStreamSynchronize(st));
     return HJ_OK;
 }

@@ -46,13 +46,15 @@ struct Req {
     uint32_t n = 0, d = 0, k = 0;
     int dtype = HJ_F32;
     double eps = 0;
-    uint64_t reserve = 0;       // bytes held while running
+    uint64_t fixed = 0;         // bytes held while running: dataset, index, operand forms
+    uint64_t allowance = 0;     // bytes held while running: the join's result buffers and results
     uint64_t result_bytes = 0;  // bytes held after completion, until collected
     int state = 0;              // 0 queued, 1 running, 2 done
     hj_status status = HJ_OK;
     char err[256] = {0};
     hj_result* result = nullptr;
     hj_join_stats stats{};
+    uint32_t regrants = 0;      // times the join asked for a larger allowance
     double t_submit = 0, t_admit = 0, t_done = 0;
 };
 
@@ -65,7 +67,8 @@ struct hj_server {
     std::deque<Req*> queue;
     std::map<uint64_t, Req*> reqs;
     uint64_t next_ticket = 1;
-    uint64_t in_use = 0;
+    uint64_t in_use = 0;        // bytes reserved by running requests and held by uncollected results
+    uint64_t peak_in_use = 0;
     uint32_t running = 0;
     bool stop = false;
     std::vector<std::thread> workers;
@@ -74,17 +77,23 @@ struct hj_server {
 
 namespace {
 
-// Device bytes one request may hold while it runs (dataset copy, index,
-// tensor-core operands and result buffers sized for ~64 neighbours per point).
-uint64_t reservation(const Req& r) {
+// Device bytes a request holds while it runs, apart from its join's result
+// buffers and results: the dataset copy, the index (points in cell order,
+// perm, cell tables and hash, workload order, work items, the sort's
+// temporaries beyond the worker's workspace) and the tensor-core operand forms.
+uint64_t fixed_bytes(const Req& r) {
     const uint64_t s = r.dtype == HJ_F64 ? 8 : 4;
     const uint64_t kpad = ((r.d + 4 + 31) / 32) * 32;
     uint64_t b = 2ull * r.n * r.d * s;          // dataset + points in cell order
-    b += 48ull * r.n;                           // perm, cell tables, workload, work items
+    b += 128ull * r.n;                          // perm, cell tables and hash, workload, sort temporaries
     if (r.dtype == HJ_F32 && r.d >= 16) b += 4ull * r.n * kpad + 16ull * r.n;   // TC operands
-    b += 64ull * r.n * 28ull;                   // pair buffers (+ band) and the result
-    return b + (64ull << 20);
+    return b + (16ull << 20);
 }
+// The first allowance for the join's result buffers and kept results: ~64
+// neighbours per point.  The join is capped at its allowance
+// (hj_join_opts.device_bytes_cap); a join that needs more is refused before it
+// allocates, and the request waits for the larger allowance it asked for.
+uint64_t first_allowance(const Req& r) { return 64ull * r.n * 28ull + (16ull << 20); }
 
 void worker_main(hj_server* S) {
     cudaSetDevice(S->device);
@@ -99,6 +108,8 @@ void worker_main(hj_server* S) {
         hj::set_current_workspace(&ws);
     } else {
         cudaGetLastError();   // no workspace: every temporary comes from the pool
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->in_use -= kWorkspaceBytes;
     }
     for (;;) {
         Req* r = nullptr;
@@ -109,13 +120,14 @@ void worker_main(hj_server* S) {
                 if (S->queue.empty()) return false;
                 const Req* f = S->queue.front();
                 // FIFO admission: the head runs when it fits, or alone when nothing else does
-                return S->running == 0 || S->in_use + f->reserve <= S->opts.hbm_budget;
+                return S->running == 0 || S->in_use + f->fixed + f->allowance <= S->opts.hbm_budget;
             });
             if (S->stop && S->queue.empty()) break;
             if (S->queue.empty()) continue;
             r = S->queue.front();
             S->queue.pop_front();
-            S->in_use += r->reserve;
+            S->in_use += r->fixed + r->allowance;
+            S->peak_in_use = std::max(S->peak_in_use, S->in_use);
             S->running++;
             r->state = 1;
             r->t_admit = now_s();
@@ -137,7 +149,28 @@ void worker_main(hj_server* S) {
             hj_join_opts_default(&o);
             o.refine = S->opts.refine;
             o.mem_fraction = 0.6 / std::max<uint32_t>(1, S->opts.workers);
+            o.device_bytes_cap = r->allowance;
             s = hj_join(ix, &o, st, &r->result, &r->stats);
+            // refused by its cap: give the allowance back, wait until the larger one it
+            // asked for fits (or nothing else runs), and join again on the same index
+            for (int tries = 0; s == HJ_ERR_OOM && r->stats.bytes_wanted > r->allowance && tries < 3; ++tries) {
+                const uint64_t want = r->stats.bytes_wanted + r->stats.bytes_wanted / 16;
+                {
+                    std::unique_lock<std::mutex> lk(S->mu);
+                    S->in_use -= r->allowance;
+                    S->running--;
+                    S->cv_work.notify_all();
+                    S->cv_work.wait(lk, [&] { return S->running == 0 || S->in_use + want <= S->opts.hbm_budget; });
+                    S->in_use += want;
+                    S->peak_in_use = std::max(S->peak_in_use, S->in_use);
+                    S->running++;
+                    r->allowance = want;
+                    r->regrants++;
+                }
+                r->err[0] = 0;
+                o.device_bytes_cap = r->allowance;
+                s = hj_join(ix, &o, st, &r->result, &r->stats);
+            }
         }
         if (s != HJ_OK && !r->err[0]) snprintf(r->err, sizeof(r->err), "%s", hj_last_error());
         if (ix) hj_index_destroy(ix);
@@ -149,7 +182,8 @@ void worker_main(hj_server* S) {
             std::lock_guard<std::mutex> lk(S->mu);
             r->status = s;
             r->result_bytes = r->result ? r->stats.total_pairs * 4ull + 16ull * r->n : 0;
-            S->in_use = S->in_use - r->reserve + r->result_bytes;
+            S->in_use = S->in_use - r->fixed - r->allowance + r->result_bytes;
+            S->peak_in_use = std::max(S->peak_in_use, S->in_use);
             S->running--;
             r->state = 2;
             r->t_done = now_s();
@@ -182,6 +216,8 @@ hj_status hj_server_create(const hj_server_opts* opts, hj_server** out) {
     if (S->opts.workers == 0) S->opts.workers = 1;
     if (S->opts.hbm_budget == 0) S->opts.hbm_budget = 150ull << 30;
     cudaGetDevice(&S->device);
+    S->in_use = (uint64_t)S->opts.workers * kWorkspaceBytes;   // the workers' workspaces
+    S->peak_in_use = S->in_use;
     for (uint32_t i = 0; i < S->opts.workers; ++i) S->workers.emplace_back(worker_main, S);
     *out = S;
     return HJ_OK;
@@ -193,7 +229,8 @@ hj_status hj_server_submit(hj_server* S, const void* h_db, uint32_t n, uint32_t 
         return HJ_ERR_INVALID;
     Req* r = new Req();
     r->h_db = h_db; r->n = n; r->d = d; r->k = k; r->dtype = dtype; r->eps = eps;
-    r->reserve = reservation(*r);
+    r->fixed = fixed_bytes(*r);
+    r->allowance = first_allowance(*r);
     r->t_submit = now_s();
     {
         std::lock_guard<std::mutex> lk(S->mu);
@@ -221,6 +258,8 @@ hj_status hj_server_wait(hj_server* S, uint64_t ticket, double timeout_s, hj_res
         info->t_admit = r->t_admit;
         info->t_done = r->t_done;
         info->stats = r->stats;
+        info->reserved_bytes = r->fixed + r->allowance;
+        info->regrants = r->regrants;
     }
     hj_status st = r->status;
     if (result) {
@@ -234,6 +273,14 @@ hj_status hj_server_wait(hj_server* S, uint64_t ticket, double timeout_s, hj_res
     lk.unlock();
     S->cv_work.notify_all();
     return st;
+}
+
+hj_status hj_server_usage(hj_server* S, uint64_t* in_use, uint64_t* peak_in_use) {
+    if (!S) return HJ_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (in_use) *in_use = S->in_use;
+    if (peak_in_use) *peak_in_use = S->peak_in_use;
+    return HJ_OK;
 }
 
 hj_status hj_server_destroy(hj_server* S) {

@@ -101,6 +101,10 @@ typedef struct {
     uint32_t keep_keys;            /* keep per-batch sorted key arrays (needed for the reference export) */
     uint32_t shard_count;          /* multi-GPU: this rank's LPT share of the work items (0 or 1 = all) */
     uint32_t shard_index;
+    uint64_t device_bytes_cap;     /* cap on the device bytes of the result buffers plus the results the
+                                      join keeps (hj_join: neighbour ids and table); 0 = none.  A join
+                                      that cannot fit returns HJ_ERR_OOM with stats->bytes_wanted set,
+                                      before its results would pass the cap */
 } hj_join_opts;
 
 typedef struct {
@@ -117,6 +121,8 @@ typedef struct {
     uint32_t refine_used;          /* HJ_REFINE_* actually used */
     uint32_t kernel_launches;      /* kernels launched by this join */
     float ms_setup;                /* workload order, refine choice, operand forms, work items (wall clock) */
+    uint64_t bytes_wanted;         /* device bytes of result buffers + kept results the join asks for by
+                                      its estimate (one batch); also filled when the cap refuses it */
 } hj_join_stats;
 
 /* ---- errors / library ---------------------------------------------------- */
@@ -289,6 +295,8 @@ typedef struct {
     hj_status status;
     double t_submit, t_admit, t_done;   /* steady-clock seconds */
     hj_join_stats stats;
+    uint64_t reserved_bytes;       /* device bytes the request held against the budget while it ran */
+    uint32_t regrants;             /* times its join asked for a larger allowance than the first */
 } hj_serve_info;
 void hj_server_opts_default(hj_server_opts* o);
 hj_status hj_server_create(const hj_server_opts* opts, hj_server** out);
@@ -300,6 +308,10 @@ hj_status hj_server_submit(hj_server* s, const void* h_db, uint32_t n, uint32_t 
  * outlive the server. */
 hj_status hj_server_wait(hj_server* s, uint64_t ticket, double timeout_s, hj_result** result,
                          hj_serve_info* info);
+/* Bytes held against the budget now (running requests' reservations, the
+ * workers' 256 MB workspaces and uncollected results) and the most ever held.
+ * A request admitted while nothing else runs may pass the budget alone. */
+hj_status hj_server_usage(hj_server* s, uint64_t* in_use, uint64_t* peak_in_use);
 hj_status hj_server_destroy(hj_server* s);
 
 /* ---- fault injection and accounting for tests --------------------------------- */
@@ -310,6 +322,9 @@ void hj_debug_fail_alloc(uint64_t nth);
 /* Bytes currently allocated from the device's default memory pool (the pool
  * every stream-ordered allocation of the library comes from). */
 hj_status hj_debug_pool_used(uint64_t* bytes);
+/* The most device memory the library's pool has held since the last reset;
+ * reset != 0 restarts the count from what is held now. */
+hj_status hj_debug_pool_peak(uint64_t* bytes, int reset);
 
 /* ---- measured peaks (roofline denominators) ---------------------------------- */
 /* Throughput of the pipes the refine kernels run on, measured by this library's

@@ -6,8 +6,9 @@
 // cpu_baseline leg load it (through oracle/__init__.py).
 //
 // Parity status: pinned against the reference itself, built from its own
-// sources by oracle/ref/Makefile (compute_80 PTX, JIT-compiled on a B200) and
-// run by oracle/ref/ref_driver.cu; the golden fixtures it produced live in
+// sources by oracle/ref/Makefile (sm_100a, with the cell-lookup comparison made
+// callable on the device) and run by oracle/ref/ref_driver.cu; the golden
+// fixtures it produced live in
 // tests/golden/ and tests/test_oracle_golden.py checks this file against them.
 //
 // Every routine cites the reference file:line whose arithmetic it restates.

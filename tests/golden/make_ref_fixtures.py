@@ -21,7 +21,7 @@ std::sort order.  A case whose largest batch could reach the reference's
 result buffer (2 x GPUBufferSize pairs, GPU.cu:1042-1062, written without a
 bounds check at kernel.cu:357-359) is skipped, never run.
 
-    python tests/golden/make_ref_fixtures.py --build        # where /root/reference exists
+    python tests/golden/make_ref_fixtures.py --build        # where the reference sources are (HJ_REFERENCE_DIR)
     python tests/golden/make_ref_fixtures.py --run OUTDIR   # on the GPU machine
 """
 from __future__ import annotations
