@@ -326,8 +326,12 @@ __device__ __forceinline__ bool warp_emit(const PairSink& s, WarpChunk& c, uint3
 // the mask counts) and its bit (n-th set bit), then calls pair_of(owner, bit).
 // Whole warp must call.  Returns false on overflow (pairs dropped; the batch
 // will be re-run).
+// With an owner value: every lane passes a value of its own (its row's id, say)
+// and pair_of(owner, bit, value of the owner lane) receives the owner's, taken
+// by a shuffle while the warp is converged.
 template <typename PairFn>
-__device__ __forceinline__ bool warp_emit_masks(const PairSink& s, WarpChunk& c, uint32_t mask, PairFn&& pair_of) {
+__device__ __forceinline__ bool warp_emit_masks_v(const PairSink& s, WarpChunk& c, uint32_t mask, uint32_t val,
+                                                  PairFn&& pair_of) {
     if (!__any_sync(0xffffffffu, mask != 0u)) return true;
     const uint32_t lane = lane_id();
     const uint32_t cnt = __popc(mask);
@@ -359,11 +363,12 @@ __device__ __forceinline__ bool warp_emit_masks(const PairSink& s, WarpChunk& c,
             const uint32_t o_incl = __shfl_sync(0xffffffffu, incl, owner);
             const uint32_t o_cnt = __shfl_sync(0xffffffffu, cnt, owner);
             const uint32_t o_mask = __shfl_sync(0xffffffffu, mask, owner);
+            const uint32_t o_val = __shfl_sync(0xffffffffu, val, owner);
             const uint32_t k = r - (o_incl - o_cnt);                  // the owner's k-th hit (0-based)
             const uint32_t bit = __fns(o_mask, 0, (int)k + 1);       // 0xFFFFFFFF if there is none
             if (b0 + lane < take && bit < 32u) {
                 const unsigned long long pos = c.base + c.used + b0 + lane;
-                const uint2 kv = pair_of(owner, bit);
+                const uint2 kv = pair_of(owner, bit, o_val);
                 s.keys[pos] = kv.x;
                 s.vals[pos] = kv.y;
             }
@@ -372,6 +377,11 @@ __device__ __forceinline__ bool warp_emit_masks(const PairSink& s, WarpChunk& c,
         done += take;
     }
     return ok;
+}
+template <typename PairFn>
+__device__ __forceinline__ bool warp_emit_masks(const PairSink& s, WarpChunk& c, uint32_t mask, PairFn&& pair_of) {
+    return warp_emit_masks_v(s, c, mask, 0u,
+                             [&](uint32_t owner, uint32_t bit, uint32_t) { return pair_of(owner, bit); });
 }
 
 }  // namespace hj

@@ -467,6 +467,7 @@ void free_index(hj_index* ix, cudaStream_t st) {
     dfree(ix->tc_a, st);
     dfree(ix->tc_b, st);
     dfree(ix->tc_err, st);
+    dfree(ix->tc_pband, st);
 }
 
 }  // namespace

@@ -62,6 +62,7 @@ struct hj_index {
     void* tc_a = nullptr;            // n x kpad, query form
     void* tc_b = nullptr;            // n x kpad, candidate form
     float* tc_err = nullptr;         // per sorted point: quantisation error norm (rounded up)
+    float* tc_pband = nullptr;       // per sorted point: its part of the guard band (rounded up)
     uint32_t tc_kpad = 0;
     int tc_kind = -1;                // HJ_REFINE_TC_F16 / _BF16 the operands hold
     void* tc_state = nullptr;        // tensor maps and error maxima (hj_refine_tc.cu)

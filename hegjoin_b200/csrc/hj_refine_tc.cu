@@ -24,7 +24,7 @@
 // with T the exact squared threshold and delta a per-candidate-row bound on
 // |D - d2_ref| (quantisation error, norm-split residual, tensor-core
 // accumulation error and the reference's own FP32 rounding; derivation in
-// tc_delta_row below).  A D that is NaN counts as "in the band", never as a
+// tc_band_p / tc_band_q below).  A D that is NaN counts as "in the band", never as a
 // reject.  The result set is therefore identical to the exact path.
 //
 // Kernel shape (one CTA per SM, persistent, 96 + 128 * EPI threads):
@@ -85,6 +85,7 @@ struct TcArgs {
     HjCellHash hash;
     HjGrid grid;
     const float4* pinfo;        // per sorted point: quantisation error norm, |x~|^2, norm-split residual
+    const float* pband;         // per sorted point: its part of the guard band (tc_band_p)
     uint32_t n;
     uint32_t nkb;               // K blocks of 32 elements
     uint32_t stages;
@@ -114,7 +115,6 @@ struct TcShared {
     uint32_t nq, ntiles, nr, q0;
     uint32_t max_e, max_n, max_r;          // float bits (non-negative)
     uint32_t qid[kQB];
-    uint32_t cidw[16 * 32];                // epilogue warp w, lane l: original id of its current row
     uint32_t rs[kMaxRanges];               // range start (sorted position)
     uint32_t rl[kMaxRanges];               // range length
     uint32_t tp[kMaxRanges + 1];           // tile prefix
@@ -134,19 +134,27 @@ struct TileWalk {
     }
 };
 
-// delta for one candidate row against the whole query block (all bounds rounded up):
+// The guard band of a candidate row c against the whole query block:
 //   |D - d2_ref| <= acc + res + e (2 sT + 3 e) + ref_rel (sT + e)^2
 //   e   = e_c + max e_q       (|x~ - x| norms; |(|q~-c~|) - |q-c|| <= e)
 //   acc = gamma (2.01 (|c~|^2 + max |q~|^2))   (tensor-core accumulation; 2|a.b| <= |a|^2 + |b|^2)
 //   res = r_c + max r_q       (norm split residuals)
-//   the last term bounds the reference's own FP32 rounding of d2 (d + 2 roundings)
-__device__ __forceinline__ float tc_delta_row(const TcArgs& a, float4 pc, float me, float mn, float mr) {
-    float e = pc.x + me;
-    float acc = a.gamma_acc * 2.01f * (pc.y + mn);
-    float r = pc.z + mr;
-    float ste = a.s_t + e;
-    float d = acc + r + e * (2.0f * a.s_t + 3.0f * e) + a.ref_rel * ste * ste;
-    return d * 1.01f + 1e-30f;
+//   the last term bounds the reference's own FP32 rounding of d2 (d + 2 roundings).
+// With (e_c + m)^2 <= 2 e_c^2 + 2 m^2 it splits into a candidate part and a
+// query-block part, delta <= P(c) + Q(block):
+//   P(c) = gamma 2.01 |c~|^2 + r_c + e_c (2 sT + 6 e_c) + ref_rel (2 sT e_c + 2 e_c^2)
+//   Q    = gamma 2.01 max|q~|^2 + max r_q + m (2 sT + 6 m) + ref_rel (sT^2 + 2 sT m + 2 m^2),  m = max e_q
+// each with a 1% margin for its own FP32 evaluation.  P is computed once per
+// point (k_tc_pband, rounded up), Q once per work item, and a row's band edges
+// are two additions rounded outwards: hi = (thr + Q) + P, lo = (thr - Q) - P.
+__host__ __device__ __forceinline__ double tc_band_p(double gamma, double s_t, double ref_rel, double e, double n2,
+                                                     double r) {
+    return (gamma * 2.01 * n2 + r + e * (2.0 * s_t + 6.0 * e) + ref_rel * (2.0 * s_t * e + 2.0 * e * e)) * 1.01;
+}
+__host__ __device__ __forceinline__ double tc_band_q(double gamma, double s_t, double ref_rel, double me, double mn,
+                                                     double mr) {
+    return (gamma * 2.01 * mn + mr + me * (2.0 * s_t + 6.0 * me) +
+            ref_rel * (s_t * s_t + 2.0 * s_t * me + 2.0 * me * me)) * 1.01 + 1e-30;
 }
 
 // Tree minimum of N values with three-input minima.  The .NaN forms return NaN
@@ -422,16 +430,21 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
             static_assert(NCH % W == 0, "whole waves per accumulator");
             const uint32_t t_first = SPLIT ? hset : 0u, t_step = SPLIT ? 2u : 1u;
             const uint32_t ncols = min((uint32_t)kAccCols, S.nq);
+            const uint32_t q0 = S.q0;
+            // the query block's part of the guard band, added to the threshold once per item
+            const float qb = __double2float_ru(tc_band_q(a.gamma_acc, a.s_t, a.ref_rel, __uint_as_float(S.max_e),
+                                                         __uint_as_float(S.max_n), __uint_as_float(S.max_r)));
+            const float thr_hi = __fadd_ru(a.thr, qb), thr_lo = __fsub_rd(a.thr, qb);
             TileWalk tw;
-            // the row's bounds and original id, loaded one tile ahead: a global load on the
-            // hit path stalls the warp, and a stalled warp holds back the release of the
+            // the row's band term and original id, loaded one tile ahead: a global load on
+            // the hit path stalls the warp, and a stalled warp holds back the release of the
             // next accumulator
-            float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+            float pb_next = 0.f;
             uint32_t cid_next = 0u;
             if (t_first < ntiles) {
                 tw.locate(S, t_first);
                 if (row < tw.valid) {
-                    pc = a.pinfo[tw.start + row];
+                    pb_next = a.pband[tw.start + row];
                     if (!a.count_only) cid_next = a.perm[tw.start + row];
                 }
             }
@@ -439,31 +452,22 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                 const uint32_t j = t & 1u;
                 const uint32_t cpos = tw.start + row;
                 const bool vrow = row < tw.valid;
-                float hi = -INFINITY, lo = -INFINITY;
-                if (vrow) {
-                    float d = tc_delta_row(a, pc, __uint_as_float(S.max_e), __uint_as_float(S.max_n),
-                                           __uint_as_float(S.max_r));
-                    hi = __fadd_ru(a.thr, d);
-                    lo = __fsub_rd(a.thr, d);
-                }
+                const float hi = vrow ? __fadd_ru(thr_hi, pb_next) : -INFINITY;
+                const float lo = vrow ? __fsub_rd(thr_lo, pb_next) : -INFINITY;
+                const uint32_t cid = cid_next;   // the owner lane's id reaches the writing lane by a shuffle
                 if (t + t_step < ntiles) {
-                    // the next tile's row bounds, loaded while this tile is processed
+                    // the next tile's rows, loaded while this tile is processed
                     tw.locate(S, t + t_step);
-                }
-                const uint32_t cid = cid_next;
-                S.cidw[ew * 32 + lane] = cid;   // read by the lanes that write this row's pairs
-                __syncwarp();
-                if (t + t_step < ntiles && row < tw.valid) {
-                    pc = a.pinfo[tw.start + row];
-                    if (!a.count_only) cid_next = a.perm[tw.start + row];
+                    if (row < tw.valid) {
+                        pb_next = a.pband[tw.start + row];
+                        if (!a.count_only) cid_next = a.perm[tw.start + row];
+                    }
                 }
                 if (!tc::mbar_wait(&S.full_acc[j], acc_use[j] & 1u, abort, a.err, a.wait_cycles)) {
                     ok = false;
                     break;
                 }
                 tc::fence_after();
-                const uint32_t* cidw = &S.cidw[ew * 32];
-                const uint32_t q0 = S.q0, cpos0 = cpos - lane;
                 if constexpr (DEFER) {
                     // fast pass: min-reduce every chunk and note, per row, the chunks with a value
                     // not above the upper band edge; no vote or branch per chunk
@@ -473,7 +477,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                         if constexpr (LDW == 64) tc::tmem_ld_32x64(tmem + lane_base + j * kAccCols + col, v);
                         else tc::tmem_ld_32x32(tmem + lane_base + j * kAccCols + col, v);
                     };
-#pragma unroll 1
+#pragma unroll
                     for (uint32_t c0 = 0; c0 < NCH; c0 += W) {
                         float v[W][LDW];
 #pragma unroll
@@ -511,11 +515,11 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                             if (a.count_only) continue;
                             // coalesced output: each lane writes every 32nd pair of the warp's
                             // hits; the owner lane's row gives the candidate
-                            warp_emit_masks(a.sink, wc_acc, amask, [&](uint32_t owner, uint32_t b) {
-                                return make_uint2(S.qid[qcol + b], cidw[owner]);
+                            warp_emit_masks_v(a.sink, wc_acc, amask, cid, [&](uint32_t, uint32_t b, uint32_t ocid) {
+                                return make_uint2(S.qid[qcol + b], ocid);
                             });
-                            warp_emit_masks(a.band, wc_band, bmask, [&](uint32_t owner, uint32_t b) {
-                                return make_uint2(q0 + qcol + b, cpos0 + owner);
+                            warp_emit_masks_v(a.band, wc_band, bmask, cpos, [&](uint32_t, uint32_t b, uint32_t opos) {
+                                return make_uint2(q0 + qcol + b, opos);
                             });
                         }
                     }
@@ -568,11 +572,11 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                                 if (a.count_only) continue;
                                 // coalesced output: each lane writes every 32nd pair of the warp's
                                 // hits; the owner lane's row gives the candidate
-                                warp_emit_masks(a.sink, wc_acc, amask, [&](uint32_t owner, uint32_t b) {
-                                    return make_uint2(S.qid[qcol + b], cidw[owner]);
+                                warp_emit_masks_v(a.sink, wc_acc, amask, cid, [&](uint32_t, uint32_t b, uint32_t ocid) {
+                                    return make_uint2(S.qid[qcol + b], ocid);
                                 });
-                                warp_emit_masks(a.band, wc_band, bmask, [&](uint32_t owner, uint32_t b) {
-                                    return make_uint2(q0 + qcol + b, cpos0 + owner);
+                                warp_emit_masks_v(a.band, wc_band, bmask, cpos, [&](uint32_t, uint32_t b, uint32_t opos) {
+                                    return make_uint2(q0 + qcol + b, opos);
                                 });
                             }
                         }
@@ -726,6 +730,15 @@ __global__ void k_tc_prep(const float* __restrict__ pts, uint32_t n, uint32_t d,
     }
 }
 
+// Each point's part of the guard band (tc_band_p), rounded up.
+__global__ void k_tc_pband(const float4* __restrict__ pinfo, uint32_t n, double gamma, double s_t, double ref_rel,
+                           float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pinfo[i];
+    out[i] = __double2float_ru(tc_band_p(gamma, s_t, ref_rel, p.x, p.y, p.z));
+}
+
 // Per-dimension minimum of the points: lanes walk a row's dimensions (coalesced
 // reads), warps stride over rows, one atomic per (block, dimension).
 __global__ void k_col_min(const float* __restrict__ pts, uint32_t n, uint32_t d, float* __restrict__ out) {
@@ -863,6 +876,14 @@ hj_status make_map(CUtensorMap* m, const void* base, uint32_t rows, uint32_t kpa
 
 uint32_t kpad_for(uint32_t d) { return ((d + 4 + 31) / 32) * 32; }
 
+// The float constants of the guard band, shared by the per-point terms and the kernel.
+float band_s_t(double thr_s) { return (float)(std::sqrt(thr_s * (1 + 1e-4)) * (1 + 1e-6)); }   // sqrt(T (1 + 1e-4))
+float band_ref_rel(uint32_t d) { return (float)((d + 2) * std::ldexp(1.0, -24) * 1.01); }
+// Accumulation model: each K=16 MMA step adds 16 exact products to the FP32
+// accumulator with at most 2 ulps of the largest magnitude per term lost
+// (alignment and truncation); bound = (steps + 1) * 32 * 2^-23 * sum|terms|.
+float band_gamma(uint32_t kpad) { return (float)((kpad / 16 + 1) * 32 * std::ldexp(1.0, -23)); }
+
 size_t tc_smem_bytes(uint32_t nkb, uint32_t stages) {
     return 1024 + (size_t)(kQT + stages) * nkb * kKBlockBytes + sizeof(TcShared);
 }
@@ -920,9 +941,8 @@ uint64_t tc_emit_warps(uint32_t nblocks) {
 
 // Half-width of the guard band for the worst pair of the dataset, in scaled units.
 static double tc_delta_scaled(const hj_index* ix, const TcState* s) {
-    double T = s->thr_s, sT = std::sqrt(T * (1 + 1e-4));
-    double e = 2.0 * s->max_e, ref = (ix->d + 2) * std::ldexp(1.0, -24) * 1.01;
-    return (s->gamma_acc * 2.01 * 2 * s->max_n + 2 * s->max_r + e * (2 * sT + 3 * e) + ref * (sT + e) * (sT + e)) * 1.01;
+    const double sT = band_s_t(s->thr_s), ref = band_ref_rel(ix->d), g = s->gamma_acc;
+    return tc_band_p(g, sT, ref, s->max_e, s->max_n, s->max_r) + tc_band_q(g, sT, ref, s->max_e, s->max_n, s->max_r);
 }
 
 // The same in the dataset's units (the figure the join reports).
@@ -981,21 +1001,25 @@ hj_status tc_prepare(hj_index* ix, int kind, cudaStream_t st) {
     dfree(ix->tc_a, st);
     dfree(ix->tc_b, st);
     dfree(ix->tc_err, st);
+    dfree(ix->tc_pband, st);
     const uint32_t kpad = kpad_for(ix->d), n = ix->n, d = ix->d;
     uint16_t *qf = nullptr, *cf = nullptr;
     float* origin = nullptr;
     float4* pinfo = nullptr;
+    float* pband = nullptr;
     unsigned long long* rng = nullptr;   // [0] max |x - origin|^2 (FP64 bits), [1] non-finite flag
     unsigned int* mx = nullptr;          // maxima of the bound terms (float bits)
     auto fail = [&](hj_status e) {
         cudaGetLastError();
         dfree(qf, st); dfree(cf, st); dfree(pinfo, st); dfree(origin, st); dfree(rng, st); dfree(mx, st);
+        dfree(pband, st);
         return e;
     };
 #define TC_TRY(x) do { hj_status e_ = (x); if (e_ != HJ_OK) return fail(e_); } while (0)
     TC_TRY(dalloc(&qf, (size_t)n * kpad, st));
     TC_TRY(dalloc(&cf, (size_t)n * kpad, st));
     TC_TRY(dalloc(&pinfo, n, st));
+    TC_TRY(dalloc(&pband, n, st));
     TC_TRY(dalloc(&origin, d, st));
     TC_TRY(dalloc(&rng, 2, st));
     TC_TRY(dalloc(&mx, 4, st));
@@ -1041,24 +1065,27 @@ hj_status tc_prepare(hj_index* ix, int kind, cudaStream_t st) {
     TcMaps maps;
     TC_TRY(make_map(&maps.query, qf, n, kpad, kind));
     TC_TRY(make_map(&maps.cand, cf, n, kpad, kind));
+    // each point's part of the guard band
+    const float gamma_acc = band_gamma(kpad);
+    const double thr_s = std::ldexp(ix->thr, 2 * sexp);
+    k_tc_pband<<<pblocks, 256, 0, st>>>(pinfo, n, gamma_acc, band_s_t(thr_s), band_ref_rel(d), pband);
+    TC_TRY(launch_status(__FILE__, __LINE__));
 #undef TC_TRY
     dfree(origin, st);
     dfree(rng, st);
     dfree(mx, st);
     TcState* s = new TcState();
     s->maps = maps;
-    // Accumulation model: each K=16 MMA step adds 16 exact products to the FP32
-    // accumulator with at most 2 ulps of the largest magnitude per term lost
-    // (alignment and truncation); bound = (steps + 1) * 32 * 2^-23 * sum|terms|.
-    s->gamma_acc = (float)((kpad / 16 + 1) * 32 * std::ldexp(1.0, -23));
+    s->gamma_acc = gamma_acc;
     s->scale_exp = sexp;
-    s->thr_s = std::ldexp(ix->thr, 2 * sexp);
+    s->thr_s = thr_s;
     std::memcpy(&s->max_e, &hm[0], 4);
     std::memcpy(&s->max_n, &hm[1], 4);
     std::memcpy(&s->max_r, &hm[2], 4);
     ix->tc_a = qf;
     ix->tc_b = cf;
     ix->tc_err = reinterpret_cast<float*>(pinfo);
+    ix->tc_pband = pband;
     ix->tc_kpad = kpad;
     ix->tc_state = s;
     ix->tc_kind = kind;
@@ -1106,11 +1133,12 @@ hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t n
     a.perm = ix->perm; a.cell_lid = ix->cell_lid; a.cell_start = ix->cell_start; a.nC = ix->nC; a.grid = ix->grid;
     a.hash = cell_hash(ix);
     a.pinfo = reinterpret_cast<const float4*>(ix->tc_err);
+    a.pband = ix->tc_pband;
     a.n = ix->n; a.nkb = nkb; a.stages = stages;
     a.thr = (float)s->thr_s;   // exact: thr * 4^s
     a.gamma_acc = s->gamma_acc;
-    a.s_t = (float)(std::sqrt(s->thr_s * (1 + 1e-4)) * (1 + 1e-6));
-    a.ref_rel = (float)((ix->d + 2) * std::ldexp(1.0, -24) * 1.01);
+    a.s_t = band_s_t(s->thr_s);
+    a.ref_rel = band_ref_rel(ix->d);
     a.sink = sink; a.band = band;
     a.count_only = count_only; a.block_counts = block_counts; a.stats = stats; a.err = err;
     a.idesc = tc::idesc_f16(ix->tc_kind == HJ_REFINE_TC_BF16 ? 1u : 0u, kTileRows, kAccCols);
