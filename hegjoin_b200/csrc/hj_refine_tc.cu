@@ -123,14 +123,23 @@ struct TcShared {
 
 // Tiles are visited in order, so the range of tile t is found by walking r
 // forward from the previous tile's range (the last r with tp[r] <= t; ranges
-// without tiles are stepped over) instead of a binary search per tile.
+// without tiles are stepped over) instead of a binary search per tile.  The
+// current range's first tile, end tile, start row and length stay in registers,
+// so a tile inside the same range costs no shared-memory reads.
 struct TileWalk {
     uint32_t r = 0, start = 0, valid = 0;
+    uint32_t t0 = 0, t1 = 0, rs = 0, rl = 0;   // range r: tiles [t0, t1), rows [rs, rs + rl)
     __device__ __forceinline__ void locate(const TcShared& S, uint32_t t) {
-        while (r + 1 < S.nr && S.tp[r + 1] <= t) ++r;
-        const uint32_t off = (t - S.tp[r]) * kTileRows;
-        start = S.rs[r] + off;
-        valid = min((uint32_t)kTileRows, S.rl[r] - off);
+        if (t >= t1) {
+            while (r + 1 < S.nr && S.tp[r + 1] <= t) ++r;
+            t0 = S.tp[r];
+            t1 = r + 1 < S.nr ? S.tp[r + 1] : 0xFFFFFFFFu;
+            rs = S.rs[r];
+            rl = S.rl[r];
+        }
+        const uint32_t off = (t - t0) * kTileRows;
+        start = rs + off;
+        valid = min((uint32_t)kTileRows, rl - off);
     }
 };
 
