@@ -103,12 +103,43 @@ __global__ void k_batch_reset(JoinCtl* c) {
 }
 
 // Number of non-sentinel keys in a sorted key array (sentinels sort last).
-__global__ void k_count_valid(const uint32_t* __restrict__ keys, unsigned long long n, unsigned long long* out) {
-    unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    bool v = keys[i] != kSentinelKey;
-    bool nxt = (i + 1 < n) && keys[i + 1] != kSentinelKey;
-    if (v && !nxt) *out = i + 1;
+// Grouping a batch's pairs by query id: a counting sort.  Keys are query ids
+// below n (sentinel slots are skipped), so one pass counts the pairs per query,
+// an exclusive scan over the n + 1 counters gives every query's first slot, and
+// one more pass scatters each pair to its query's run.  Lanes of a warp holding
+// the same key share one atomic (a leader adds the group's size).  Within a
+// query the order of its pairs is not defined, as in the reference (whose key
+// sort is unstable).
+__global__ void k_group_count(const uint32_t* __restrict__ keys, unsigned long long m, uint32_t* __restrict__ cnt) {
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
+         base += stride) {
+        const unsigned long long i = base + lane_id();
+        const uint32_t key = i < m ? keys[i] : kSentinelKey;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (key != kSentinelKey && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&cnt[key], __popc(peers));
+    }
+}
+
+__global__ void k_group_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                unsigned long long m, uint32_t* __restrict__ cursor, uint32_t* __restrict__ keys_out,
+                                uint32_t* __restrict__ vals_out) {
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
+         base += stride) {
+        const unsigned long long i = base + lane_id();
+        const uint32_t key = i < m ? keys[i] : kSentinelKey;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t first = 0;
+        if (key != kSentinelKey && lane_id() == leader) first = atomicAdd(&cursor[key], __popc(peers));
+        first = __shfl_sync(0xffffffffu, first, leader);
+        if (key != kSentinelKey) {
+            const uint32_t pos = first + __popc(peers & lanemask_lt());
+            keys_out[pos] = key;
+            vals_out[pos] = vals[i];
+        }
+    }
 }
 
 __device__ __forceinline__ unsigned long long lower_bound_u32(const uint32_t* a, unsigned long long n, uint32_t v) {
@@ -640,7 +671,8 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     uint32_t *keys = slab, *vals = slab + cap, *keys_tmp = slab + 2 * cap, *vals_tmp = slab + 3 * cap;
     uint32_t* band_q = tc ? slab + 4 * cap : nullptr;
     uint32_t* band_c = tc ? slab + 5 * cap : nullptr;
-    const uint32_t key_bits = bits_for(ix->n);
+    uint32_t* qoff = nullptr;   // per-query counters, then first slots, of the grouping
+    HJ_TRY(tmp.alloc(&qoff, (size_t)ix->n + 1));
 
     auto t_ref = std::chrono::steady_clock::now();
     float ms_group = 0;
@@ -681,13 +713,18 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             continue;
         }
         auto t_g = std::chrono::steady_clock::now();
-        uint64_t slots = std::min<uint64_t>(used, cap);
-        HJ_TRY(radix_sort_u32_u32(keys, vals, keys_tmp, vals_tmp, slots, key_bits, st));
-        unsigned long long valid = 0;
+        const uint64_t slots = std::min<uint64_t>(used, cap);
+        uint32_t valid = 0;
         if (slots) {
-            k_count_valid<<<(unsigned)((slots + 255) / 256), 256, 0, st>>>(keys, slots, &ctl->valid);
+            // group by query id: count, scan (qoff[n] = the batch's pairs), scatter into the copies
+            HJ_CUDA(cudaMemsetAsync(qoff, 0, ((size_t)ix->n + 1) * 4, st));
+            const unsigned g = (unsigned)std::min<uint64_t>((slots + 255) / 256, (uint64_t)num_sms() * 16);
+            k_group_count<<<g, 256, 0, st>>>(keys, slots, qoff);
             HJ_LAUNCHED();
-            HJ_CUDA(cudaMemcpyAsync(&valid, &ctl->valid, 8, cudaMemcpyDeviceToHost, st));
+            HJ_TRY(scan_u32_inplace(qoff, (uint64_t)ix->n + 1, st));
+            HJ_CUDA(cudaMemcpyAsync(&valid, qoff + ix->n, 4, cudaMemcpyDeviceToHost, st));
+            k_group_scatter<<<g, 256, 0, st>>>(keys, vals, slots, qoff, keys_tmp, vals_tmp);
+            HJ_LAUNCHED();
             HJ_CUDA(cudaStreamSynchronize(st));
         }
         if (cap_bytes && kept + kept_bytes_per_pair * (double)valid > (double)cap_bytes) {
@@ -705,7 +742,7 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             return HJ_ERR_OOM;
         }
         kept += kept_bytes_per_pair * (double)valid;
-        HJ_TRY(handler.on_batch(n_out, keys, vals, valid, st));
+        HJ_TRY(handler.on_batch(n_out, keys_tmp, vals_tmp, valid, st));
         ++n_out;
         total += valid;
         ms_group += ms_since(t_g);
