@@ -205,6 +205,8 @@ inline uint32_t bits_for(uint64_t max_value) {
 hj_status scan_u32_to_u64(const uint32_t* in, uint64_t* out, uint64_t n, cudaStream_t st);
 // In-place exclusive scan of u32 values (total must fit in u32).
 hj_status scan_u32_inplace(uint32_t* data, uint64_t n, cudaStream_t st);
+// In-place exclusive scan of doubles.
+hj_status scan_f64_inplace(double* data, uint64_t n, cudaStream_t st);
 // Stable LSD radix sort of (key, value) pairs on the low `nbits` key bits.
 // On return the sorted data is in (keys, vals) (tmp buffers are scratch of n).
 hj_status radix_sort_u64_u32(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp,

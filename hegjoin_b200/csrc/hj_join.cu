@@ -78,6 +78,70 @@ __global__ void k_pick_samples(const HjBlock* __restrict__ blocks, uint32_t nblo
     out[i] = blocks[min(nblocks - 1, i * stride)];
 }
 
+// Estimated pairs per work item, on the device: the sampled rate (pairs per
+// query) of the item's sample group, or the larger of its group's and the next
+// group's for items between samples, times the item's queries
+// (GPUBatchEst_v2's extrapolation, GPU.cu:608-633, on work items); est[nblocks]
+// = 0 for the exclusive scan.  Queries x candidates of every item add up in *cand.
+__global__ void k_item_estimates(const HjBlock* __restrict__ blocks, uint32_t nblocks, uint32_t stride,
+                                 uint32_t nsamp, const HjBlock* __restrict__ sblocks,
+                                 const unsigned long long* __restrict__ scnt, double* __restrict__ est,
+                                 double* __restrict__ cand) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double c = 0;
+    if (i < nblocks) {
+        const uint32_t s = min(i / stride, nsamp - 1);
+        auto rate = [&](uint32_t q) { return (double)scnt[q] / (double)max(1u, sblocks[q].q1 - sblocks[q].q0); };
+        double r = rate(s);
+        if (i % stride != 0) r = fmax(r, rate(min(nsamp - 1, s + 1)));
+        const HjBlock b = blocks[i];
+        est[i] = r * (double)(b.q1 - b.q0);
+        c = (double)b.nb * (double)(b.q1 - b.q0);
+    } else if (i == nblocks) {
+        est[i] = 0;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if (lane_id() == 0 && c > 0) atomicAdd(cand, c);
+}
+
+// Batch cuts: item i > 0 starts a batch where the exclusive prefix of the
+// estimates crosses a multiple of the budget, so a batch's estimate stays below
+// the budget plus its last item's.
+__global__ void k_batch_cuts(const double* __restrict__ pre, uint32_t nblocks, double budget,
+                             uint32_t* __restrict__ cuts, unsigned int* __restrict__ ncuts) {
+    const uint32_t i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nblocks) return;
+    if (floor(pre[i] / budget) != floor(pre[i - 1] / budget)) cuts[atomicAdd(ncuts, 1u)] = i;
+}
+
+// Light work items (at most kLightCandidates candidates per query) go in cell
+// order.  The workload order runs the heavy items first, which keeps the
+// persistent refine balanced, but it scatters the many light items of sparse
+// data over the whole grid: spatial neighbours, which read the same candidate
+// cells and probe the same hash slots, then run far apart and miss in L2.  In
+// cell (linear id) order consecutive light items share most of their stencil.
+constexpr uint32_t kLightCandidates = 4096;
+
+// Items whose cells have more candidates than `lim`: a prefix, since the items
+// follow the workload order (candidates non-increasing).
+__global__ void k_count_heavy(const HjBlock* __restrict__ b, uint32_t n, uint32_t lim, unsigned int* cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t heavy = __popc(__ballot_sync(0xffffffffu, i < n && b[i].nb > lim));
+    if (lane_id() == 0 && heavy) atomicAdd(cnt, heavy);
+}
+__global__ void k_item_cells(const HjBlock* __restrict__ b, uint32_t m, uint32_t* __restrict__ cell,
+                             uint32_t* __restrict__ idx) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    cell[i] = b[i].cell;
+    idx[i] = i;
+}
+__global__ void k_gather_items(const HjBlock* __restrict__ in, const uint32_t* __restrict__ idx, uint32_t m,
+                               HjBlock* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = in[idx[i]];
+}
+
 // Counters and flags of one join, in one device allocation.
 struct JoinCtl {
     unsigned long long cursor;        // pair sink cursor of the current batch
@@ -301,41 +365,89 @@ __global__ void k_pick_list(const HjBlock* __restrict__ blocks, const uint32_t* 
     if (i < m) out[i] = blocks[items[i]];
 }
 
-// Per-query digest of one grouped batch, added into (count, sum, xor): warps
-// take 32 consecutive pairs, reduce each run of equal query ids with a
-// segmented scan, and the last lane of a run adds it with three atomics.
-__global__ void k_digest_accumulate(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                                    unsigned long long n, uint32_t* __restrict__ cnt,
-                                    unsigned long long* __restrict__ sum, unsigned long long* __restrict__ xr) {
-    const uint32_t lane = lane_id();
+// Per-query digests of a grouped batch (keys ascending): (count, sum of
+// mix64(id), xor of mix64(id ^ salt)) per query, added into (cnt, sum, xr).  A
+// warp stages a walk of 512 consecutive pairs in shared memory (coalesced loads)
+// and every lane folds its 16 consecutive ones serially.  Runs that begin and
+// end inside a lane go out with one atomic triple.  A lane's last run may go on
+// in the next lanes: a segmented scan over the lanes' last runs (equal keys
+// chain; a lane whose last run continues the previous lane's holds one key
+// only) gives each run's total up to every lane; the lane where the run ends
+// writes it, or, when the next lane's first run continues it and that lane
+// holds more runs, that lane adds its first run and writes it.  Long runs (a
+// query with thousands of neighbours) cost one scan and a few atomics per 512
+// pairs; a run crossing two walks is written by both (the digest adds up).
+constexpr uint32_t kDigestPer = 16;                  // pairs per lane per walk
+constexpr uint32_t kDigestSpan = 32 * kDigestPer;    // pairs per warp per walk
+__device__ __forceinline__ void digest_out(uint32_t* cnt, unsigned long long* sum, unsigned long long* xr,
+                                           uint32_t key, uint32_t c, unsigned long long s, unsigned long long x) {
+    atomicAdd(&cnt[key], c);
+    atomicAdd(&sum[key], s);
+    atomicXor(&xr[key], x);
+}
+__global__ void __launch_bounds__(256) k_digest_accumulate(const uint32_t* __restrict__ keys,
+                                                            const uint32_t* __restrict__ vals, unsigned long long n,
+                                                            uint32_t* __restrict__ cnt, unsigned long long* __restrict__ sum,
+                                                            unsigned long long* __restrict__ xr) {
+    // per warp: the walk's keys and values, 16 per lane with one word of padding per lane
+    // so that the lanes' serial reads fall in different banks
+    __shared__ uint32_t sk[8][32 * (kDigestPer + 1)], sv[8][32 * (kDigestPer + 1)];
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
     const unsigned long long warps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
-    for (unsigned long long base = (((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32ull;
-         base < n; base += warps * 32ull) {
-        const unsigned long long i = base + lane;
-        const bool valid = i < n;
-        const uint32_t key = valid ? keys[i] : kSentinelKey;
-        const uint32_t v = valid ? vals[i] : 0u;
-        unsigned long long s = valid ? mix64(v) : 0ull;
-        unsigned long long x = valid ? mix64((uint64_t)v ^ 0x5bd1e9955bd1e995ull) : 0ull;
-        uint32_t c = valid ? 1u : 0u;
+    for (unsigned long long base = (((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kDigestSpan;
+         base < n; base += warps * kDigestSpan) {
+#pragma unroll
+        for (uint32_t j = 0; j < kDigestPer; ++j) {
+            const uint32_t e = j * 32 + lane;                          // element of the walk
+            const uint32_t slot = (e / kDigestPer) * (kDigestPer + 1) + e % kDigestPer;
+            const unsigned long long i = base + e;
+            sk[w][slot] = i < n ? keys[i] : kSentinelKey;
+            sv[w][slot] = i < n ? vals[i] : 0u;
+        }
+        __syncwarp();
+        const uint32_t* mk = &sk[w][lane * (kDigestPer + 1)];
+        const uint32_t* mv = &sv[w][lane * (kDigestPer + 1)];
+        uint32_t fk = kSentinelKey, fc = 0, lk = mk[0], lc = 0;
+        unsigned long long fs = 0, fx = 0, ls = 0, lx = 0;
+        bool single = true;
+#pragma unroll 4
+        for (uint32_t j = 0; j < kDigestPer; ++j) {
+            const uint32_t key = mk[j];
+            if (key == kSentinelKey) break;   // sentinels only trail
+            if (key != lk) {
+                if (single) { fk = lk; fc = lc; fs = ls; fx = lx; single = false; }
+                else digest_out(cnt, sum, xr, lk, lc, ls, lx);
+                lk = key; lc = 0; ls = 0; lx = 0;
+            }
+            const uint32_t v = mv[j];
+            lc += 1;
+            ls += mix64(v);
+            lx ^= mix64((uint64_t)v ^ 0x5bd1e9955bd1e995ull);
+        }
+        const uint32_t key_first = single ? lk : fk;
+        // segmented scan of the last runs over the lanes
+        unsigned long long s = ls, x = lx;
+        uint32_t c = lc;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t k2 = __shfl_up_sync(0xffffffffu, key, o);
+            const uint32_t k2 = __shfl_up_sync(0xffffffffu, lk, o);
             const unsigned long long s2 = __shfl_up_sync(0xffffffffu, s, o);
             const unsigned long long x2 = __shfl_up_sync(0xffffffffu, x, o);
             const uint32_t c2 = __shfl_up_sync(0xffffffffu, c, o);
-            if (lane >= (uint32_t)o && k2 == key) {   // keys are sorted: equal keys are contiguous
-                s += s2;
-                x ^= x2;
-                c += c2;
-            }
+            if (lane >= (uint32_t)o && k2 == lk) { s += s2; x ^= x2; c += c2; }
         }
-        const uint32_t next = __shfl_down_sync(0xffffffffu, key, 1);
-        if (valid && (lane == 31 || next != key)) {
-            atomicAdd(&cnt[key], c);
-            atomicAdd(&sum[key], s);
-            atomicXor(&xr[key], x);
+        const uint32_t pk = __shfl_up_sync(0xffffffffu, lk, 1);
+        const unsigned long long ps = __shfl_up_sync(0xffffffffu, s, 1), px = __shfl_up_sync(0xffffffffu, x, 1);
+        const uint32_t pc = __shfl_up_sync(0xffffffffu, c, 1);
+        const uint32_t nk = __shfl_down_sync(0xffffffffu, key_first, 1);
+        if (!single) {
+            // the first run: complete here, joined with the previous lanes' run when it goes on from there
+            if (lane > 0 && pk == fk) digest_out(cnt, sum, xr, fk, fc + pc, fs + ps, fx ^ px);
+            else digest_out(cnt, sum, xr, fk, fc, fs, fx);
         }
+        // the last run (with its earlier lanes) ends here unless the next lane goes on with it
+        if (lk != kSentinelKey && (lane == 31 || nk != lk)) digest_out(cnt, sum, xr, lk, c, s, x);
+        __syncwarp();
     }
 }
 
@@ -433,12 +545,47 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     uint32_t nblocks = 0;
     HJ_TRY(build_blocks(ix, qb, &blocks, &nblocks, st));
     tmp.adopt(blocks);
-    std::vector<HjBlock> hblocks(nblocks);
-    if (nblocks) {
-        HJ_CUDA(cudaMemcpyAsync(hblocks.data(), blocks, (size_t)nblocks * sizeof(HjBlock), cudaMemcpyDeviceToHost, st));
+    if (!tc && nblocks > 1) {
+        // the light items' tail in cell order (kLightCandidates)
+        unsigned int* dh = nullptr;
+        HJ_TRY(tmp.alloc(&dh, 1));
+        HJ_CUDA(cudaMemsetAsync(dh, 0, sizeof(unsigned int), st));
+        k_count_heavy<<<(nblocks + 255) / 256, 256, 0, st>>>(blocks, nblocks, kLightCandidates, dh);
+        HJ_LAUNCHED();
+        unsigned int heavy = 0;
+        HJ_CUDA(cudaMemcpyAsync(&heavy, dh, sizeof(heavy), cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
+        tmp.release(dh);
+        const uint32_t m = nblocks - heavy;
+        if (m > 1) {
+            uint32_t *cell = nullptr, *idx = nullptr, *cell_t = nullptr, *idx_t = nullptr;
+            HjBlock* out = nullptr;
+            HJ_TRY(tmp.alloc(&cell, m));
+            HJ_TRY(tmp.alloc(&idx, m));
+            HJ_TRY(tmp.alloc(&cell_t, m));
+            HJ_TRY(tmp.alloc(&idx_t, m));
+            HJ_TRY(tmp.alloc(&out, m));
+            k_item_cells<<<(m + 255) / 256, 256, 0, st>>>(blocks + heavy, m, cell, idx);
+            HJ_LAUNCHED();
+            HJ_TRY(radix_sort_u32_u32(cell, idx, cell_t, idx_t, m, bits_for(ix->nC), st));
+            k_gather_items<<<(m + 255) / 256, 256, 0, st>>>(blocks + heavy, idx, m, out);
+            HJ_LAUNCHED();
+            HJ_CUDA(cudaMemcpyAsync(blocks + heavy, out, (size_t)m * sizeof(HjBlock), cudaMemcpyDeviceToDevice, st));
+            tmp.release(out);
+            tmp.release(idx_t);
+            tmp.release(cell_t);
+            tmp.release(idx);
+            tmp.release(cell);
+        }
     }
     if (opts.shard_count > 1) {
+        // the item list on the host, for the costs of the share
+        std::vector<HjBlock> hblocks(nblocks);
+        if (nblocks) {
+            HJ_CUDA(cudaMemcpyAsync(hblocks.data(), blocks, (size_t)nblocks * sizeof(HjBlock), cudaMemcpyDeviceToHost,
+                                    st));
+            HJ_CUDA(cudaStreamSynchronize(st));
+        }
         // this rank's share of the items: greedy LPT on (candidates x queries) per item
         std::vector<uint64_t> cost(nblocks);
         for (uint32_t i = 0; i < nblocks; ++i) cost[i] = (uint64_t)hblocks[i].nb * (hblocks[i].q1 - hblocks[i].q0);
@@ -454,9 +601,6 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             k_pick_list<<<(n_mine + 255) / 256, 256, 0, st>>>(blocks, d_items, n_mine, sel);
             HJ_LAUNCHED();
         }
-        std::vector<HjBlock> hsel(n_mine);
-        for (uint32_t i = 0; i < n_mine; ++i) hsel[i] = hblocks[mine[i]];
-        hblocks.swap(hsel);
         HJ_CUDA(cudaStreamSynchronize(st));   // the host copy of the item list is read by the copy above
         tmp.release(blocks);
         tmp.release(d_items);
@@ -509,8 +653,9 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     S.ms_setup = ms_since(t_start);
     uint32_t stride = std::max<uint32_t>(1, (uint32_t)std::lround(1.0 / opts.sample_rate));
     uint32_t nsamp = nblocks ? (nblocks + stride - 1) / stride : 0;
-    std::vector<double> est(nblocks, 0.0);
-    double total_est = 0;
+    double total_est = 0, cand_total = 0;
+    double* pest = nullptr;   // exclusive prefix of the per-item estimates (nblocks + 1)
+    double* dsum = nullptr;
     if (nsamp) {
         HjBlock* sblocks = nullptr;
         unsigned long long* scnt = nullptr;
@@ -529,14 +674,15 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             HJ_TRY(check_timeout());
             {
                 std::vector<unsigned long long> h0(nsamp);
+                std::vector<HjBlock> hs0(nsamp);
                 HJ_CUDA(cudaMemcpyAsync(h0.data(), scnt, nsamp * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                         st));
+                HJ_CUDA(cudaMemcpyAsync(hs0.data(), sblocks, nsamp * sizeof(HjBlock), cudaMemcpyDeviceToHost, st));
                 HJ_CUDA(cudaStreamSynchronize(st));
                 double sp = 0, sc = 0;
                 for (uint32_t q = 0; q < nsamp; ++q) {
-                    const HjBlock& b = hblocks[std::min(nblocks - 1, q * stride)];
                     sp += (double)h0[q];
-                    sc += (double)b.nb * (b.q1 - b.q0);
+                    sc += (double)hs0[q].nb * (hs0[q].q1 - hs0[q].q0);
                 }
                 tc_set_defer(ix, defer_for(sp, sc));
             }
@@ -567,30 +713,25 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
             HJ_TRY(check_timeout());
         }
-        std::vector<unsigned long long> hs(nsamp);
-        HJ_CUDA(cudaMemcpyAsync(hs.data(), scnt, nsamp * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        // per-item estimates and their exclusive prefix on the device; the host reads the
+        // totals only (the item list of a sparse dataset runs to millions of entries)
+        HJ_TRY(tmp.alloc(&pest, (size_t)nblocks + 1));
+        HJ_TRY(tmp.alloc(&dsum, 1));
+        HJ_CUDA(cudaMemsetAsync(dsum, 0, sizeof(double), st));
+        k_item_estimates<<<(nblocks + 256) / 256, 256, 0, st>>>(blocks, nblocks, stride, nsamp, sblocks, scnt, pest,
+                                                                 dsum);
+        HJ_LAUNCHED();
+        HJ_TRY(scan_f64_inplace(pest, (uint64_t)nblocks + 1, st));
+        double hsum[2] = {0, 0};
+        HJ_CUDA(cudaMemcpyAsync(&hsum[0], pest + nblocks, sizeof(double), cudaMemcpyDeviceToHost, st));
+        HJ_CUDA(cudaMemcpyAsync(&hsum[1], dsum, sizeof(double), cudaMemcpyDeviceToHost, st));
         HJ_CUDA(cudaStreamSynchronize(st));
-        tmp.release(sblocks);
-        tmp.release(scnt);
-        std::vector<double> rate(nsamp);
-        for (uint32_t s = 0; s < nsamp; ++s) {
-            const HjBlock& b = hblocks[std::min(nblocks - 1, s * stride)];
-            rate[s] = (double)hs[s] / std::max<uint32_t>(1, b.q1 - b.q0);
-        }
-        for (uint32_t i = 0; i < nblocks; ++i) {
-            uint32_t s = i / stride;
-            double r = (i % stride == 0) ? rate[s] : std::max(rate[s], rate[std::min(nsamp - 1, s + 1)]);
-            est[i] = r * (hblocks[i].q1 - hblocks[i].q0);
-            total_est += est[i];
-        }
+        total_est = hsum[0];
+        cand_total = hsum[1];
     }
     S.estimated_pairs = (uint64_t)total_est;
     S.ms_estimate = ms_since(t_est);
-    if (tc) {
-        double cand = 0;
-        for (uint32_t i = 0; i < nblocks; ++i) cand += (double)hblocks[i].nb * (hblocks[i].q1 - hblocks[i].q0);
-        tc_set_defer(ix, defer_for(total_est, cand));
-    }
+    if (tc) tc_set_defer(ix, defer_for(total_est, cand_total));
 
     // ---- result buffer capacity
     // slack for partly filled warp chunks: every warp that can emit during a batch holds
@@ -639,19 +780,33 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
 
     // ---- batches: cut the workload order at half the buffer by estimate
     std::vector<Batch> batches;
-    {
-        double budget = 0.5 * (double)(cap - chunk_slack);
-        uint32_t b0 = 0;
-        double run = 0;
-        for (uint32_t i = 0; i < nblocks; ++i) {
-            if (run > 0 && run + est[i] > budget) {
-                batches.push_back({b0, i});
-                b0 = i;
-                run = 0;
+    if (nblocks) {
+        const double budget = 0.5 * (double)(cap - chunk_slack);
+        std::vector<uint32_t> cuts;
+        if (nblocks > 1 && total_est >= budget) {
+            uint32_t* dcuts = nullptr;
+            unsigned int* dn = nullptr;
+            HJ_TRY(tmp.alloc(&dcuts, nblocks));
+            HJ_TRY(tmp.alloc(&dn, 1));
+            HJ_CUDA(cudaMemsetAsync(dn, 0, sizeof(unsigned int), st));
+            k_batch_cuts<<<(nblocks + 254) / 256, 256, 0, st>>>(pest, nblocks, budget, dcuts, dn);
+            HJ_LAUNCHED();
+            unsigned int ncut = 0;
+            HJ_CUDA(cudaMemcpyAsync(&ncut, dn, sizeof(ncut), cudaMemcpyDeviceToHost, st));
+            HJ_CUDA(cudaStreamSynchronize(st));
+            cuts.resize(ncut);
+            if (ncut) {
+                HJ_CUDA(cudaMemcpyAsync(cuts.data(), dcuts, (size_t)ncut * 4, cudaMemcpyDeviceToHost, st));
+                HJ_CUDA(cudaStreamSynchronize(st));
             }
-            run += est[i];
+            std::sort(cuts.begin(), cuts.end());
         }
-        if (b0 < nblocks) batches.push_back({b0, nblocks});
+        uint32_t b0 = 0;
+        for (uint32_t c : cuts) {
+            batches.push_back({b0, c});
+            b0 = c;
+        }
+        batches.push_back({b0, nblocks});
     }
     std::reverse(batches.begin(), batches.end());   // used as a stack
 
@@ -813,7 +968,8 @@ struct StreamHandler : BatchHandler {
     hj_status on_batch(uint32_t bi, const uint32_t* keys, const uint32_t* vals, uint64_t count,
                        cudaStream_t st) override {
         if (count && cnt) {
-            const unsigned g = (unsigned)std::min<uint64_t>((count + 255) / 256, (uint64_t)num_sms() * 16);
+            const uint64_t per_block = 8ull * kDigestSpan;   // 8 warps, each a walk of 512 pairs
+            const unsigned g = (unsigned)std::min<uint64_t>((count + per_block - 1) / per_block, (uint64_t)num_sms() * 16);
             k_digest_accumulate<<<g, 256, 0, st>>>(keys, vals, count, cnt, sum, xr);
             HJ_LAUNCHED();
         }

@@ -249,6 +249,9 @@ hj_status scan_u32_to_u64(const uint32_t* in, uint64_t* out, uint64_t n, cudaStr
 hj_status scan_u32_inplace(uint32_t* data, uint64_t n, cudaStream_t st) {
     return exclusive_scan<uint32_t, uint32_t>(data, data, n, st);
 }
+hj_status scan_f64_inplace(double* data, uint64_t n, cudaStream_t st) {
+    return exclusive_scan<double, double>(data, data, n, st);
+}
 hj_status radix_sort_u64_u32(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, uint64_t n,
                              uint32_t nbits, cudaStream_t st) {
     return radix_sort<uint64_t>(keys, vals, keys_tmp, vals_tmp, n, nbits, st);
