@@ -524,7 +524,7 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     bool tc = refine == HJ_REFINE_TC_F16 || refine == HJ_REFINE_TC_BF16;
     if (tc) {
         if (!tc_supported(ix, refine)) {
-            set_error("hj_join: the tensor-core filter needs float data with 16 <= d <= %d", 252);
+            set_error("hj_join: the tensor-core filter needs float data with 8 <= d <= 188 and k <= 6");
             return HJ_ERR_UNSUPPORTED;
         }
         const hj_status ps = tc_prepare(ix, refine, st);
