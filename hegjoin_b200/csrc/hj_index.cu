@@ -421,16 +421,34 @@ hj_status index_create_t(const T* d_db, uint32_t n, uint32_t d, uint32_t k, T ep
     return HJ_OK;
 }
 
-__global__ void k_hash_insert(const unsigned long long* __restrict__ lid, uint32_t nC, unsigned long long* keys,
-                              uint32_t* vals, unsigned long long mask) {
+// Cells that open a group (the first of their lid >> 2): their number, for the
+// capacity.
+__global__ void k_count_groups(const unsigned long long* __restrict__ lid, uint32_t nC, unsigned int* groups) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool opens = i < nC && (i == 0 || (lid[i - 1] >> 2) != (lid[i] >> 2));
+    const uint32_t c = __popc(__ballot_sync(0xffffffffu, opens));
+    if (lane_id() == 0 && c) atomicAdd(groups, c);
+}
+
+// The first cell of each group inserts the group's entry: key, first cell, mask
+// of the group's ids (its cells are the next ones in the table, at most four).
+// The key word pair is claimed with a 64-bit compare-and-swap on the entry's
+// first 8 bytes; first cell and mask are written after it.
+__global__ void k_hash_insert(const unsigned long long* __restrict__ lid, uint32_t nC, uint4* entries,
+                              unsigned long long mask) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nC) return;
-    const unsigned long long key = lid[i];
-    unsigned long long s = mix64(key) & mask;
+    const unsigned long long g = lid[i] >> 2;
+    if (i > 0 && (lid[i - 1] >> 2) == g) return;
+    uint32_t m = 0;
+    for (uint32_t j = i; j < nC && j < i + 4 && (lid[j] >> 2) == g; ++j) m |= 1u << (uint32_t)(lid[j] & 3u);
+    unsigned long long s = mix64(g) & mask;
     for (unsigned long long probe = 0; probe <= mask; ++probe) {   // the table is at most half full
-        const unsigned long long prev = atomicCAS(&keys[s], kEmptyLid, key);
-        if (prev == kEmptyLid || prev == key) {
-            vals[s] = i;
+        unsigned long long* kw = reinterpret_cast<unsigned long long*>(&entries[s]);
+        const unsigned long long prev = atomicCAS(kw, kEmptyLid, g);
+        if (prev == kEmptyLid) {
+            entries[s].z = i;
+            entries[s].w = m;
             return;
         }
         s = (s + 1) & mask;
@@ -438,17 +456,28 @@ __global__ void k_hash_insert(const unsigned long long* __restrict__ lid, uint32
 }
 
 // The cell hash of an index whose cell table is built (capacity: the power of
-// two at least twice nC, at least 64).
+// two at least twice the number of groups, at least 64).
 hj_status build_cell_hash(hj_index* ix, cudaStream_t st) {
+    unsigned long long groups = 0;
+    if (ix->nC) {
+        Scratch tmp(st);
+        unsigned int* dg = nullptr;
+        HJ_TRY(tmp.alloc(&dg, 1));
+        HJ_CUDA(cudaMemsetAsync(dg, 0, sizeof(unsigned int), st));
+        k_count_groups<<<(ix->nC + 255) / 256, 256, 0, st>>>(ix->cell_lid, ix->nC, dg);
+        HJ_LAUNCHED();
+        unsigned int hg = 0;
+        HJ_CUDA(cudaMemcpyAsync(&hg, dg, sizeof(hg), cudaMemcpyDeviceToHost, st));
+        HJ_CUDA(cudaStreamSynchronize(st));
+        groups = hg;
+    }
     unsigned long long cap = 64;
-    while (cap < 2ull * ix->nC) cap <<= 1;
-    HJ_TRY(dalloc(&ix->hash_keys, (size_t)cap, st));
-    HJ_TRY(dalloc(&ix->hash_vals, (size_t)cap, st));
-    HJ_CUDA(cudaMemsetAsync(ix->hash_keys, 0xFF, (size_t)cap * sizeof(unsigned long long), st));
+    while (cap < 2ull * groups) cap <<= 1;
+    HJ_TRY(dalloc(&ix->hash_entries, (size_t)cap, st));
+    HJ_CUDA(cudaMemsetAsync(ix->hash_entries, 0xFF, (size_t)cap * sizeof(uint4), st));
     ix->hash_mask = cap - 1;
     if (ix->nC) {
-        k_hash_insert<<<(ix->nC + 255) / 256, 256, 0, st>>>(ix->cell_lid, ix->nC, ix->hash_keys, ix->hash_vals,
-                                                             ix->hash_mask);
+        k_hash_insert<<<(ix->nC + 255) / 256, 256, 0, st>>>(ix->cell_lid, ix->nC, ix->hash_entries, ix->hash_mask);
         HJ_LAUNCHED();
     }
     return HJ_OK;
@@ -456,8 +485,7 @@ hj_status build_cell_hash(hj_index* ix, cudaStream_t st) {
 
 void free_index(hj_index* ix, cudaStream_t st) {
     tc_release(ix);
-    dfree(ix->hash_keys, st);
-    dfree(ix->hash_vals, st);
+    dfree(ix->hash_entries, st);
     dfree(ix->pts, st);
     dfree(ix->perm, st);
     dfree(ix->cell_lid, st);

@@ -10,13 +10,18 @@ struct HjGrid {
     unsigned long long mult[hj::kMaxK];   // mixed-radix multipliers, dimension 0 fastest
 };
 
-// Open-addressing hash of the non-empty cells, linear id -> cell index, so a
-// stencil row is found with one or two loads instead of a binary search over
-// all non-empty cells.  Capacity is a power of two at least twice nC; free
-// slots hold kEmptyLid (no cell can have that id: the index rejects it).
+// Open-addressing hash of the non-empty cells, keyed by groups of four
+// consecutive linear ids (g = lid >> 2).  An entry is 16 bytes: the group key
+// (two words), the cell index of the group's first non-empty cell, and a 4-bit
+// mask of the group's non-empty ids; the group's cells are consecutive in the
+// cell table (sorted by linear id), so the cell of id g*4 + b is the first cell
+// plus the number of mask bits below b.  A stencil row (up to 3 consecutive ids
+// along dimension 0) spans one or two groups: one or two 16-byte loads, and
+// neighbouring cells along dimension 0 hit the same entries.  Capacity is a
+// power of two at least twice the number of groups; free entries hold the key
+// kEmptyLid (no group can have it: linear ids stay below 2^63).
 struct HjCellHash {
-    const unsigned long long* keys;
-    const uint32_t* vals;
+    const uint4* entries;
     unsigned long long mask;   // capacity - 1
 };
 
@@ -47,8 +52,7 @@ struct hj_index {
     unsigned long long* cell_lid = nullptr;  // nC sorted linear ids
     uint32_t* cell_start = nullptr;  // nC + 1
     uint32_t nC = 0;
-    unsigned long long* hash_keys = nullptr;   // cell hash (HjCellHash)
-    uint32_t* hash_vals = nullptr;
+    uint4* hash_entries = nullptr;   // cell hash (HjCellHash)
     unsigned long long hash_mask = 0;
 
     // workload (hj_sort_by_workload)
@@ -86,7 +90,7 @@ hj_status build_blocks(const hj_index* ix, uint32_t qb, HjBlock** d_blocks, uint
 constexpr unsigned long long kEmptyLid = ~0ull;
 constexpr uint32_t kNoCell = 0xFFFFFFFFu;
 
-inline HjCellHash cell_hash(const hj_index* ix) { return HjCellHash{ix->hash_keys, ix->hash_vals, ix->hash_mask}; }
+inline HjCellHash cell_hash(const hj_index* ix) { return HjCellHash{ix->hash_entries, ix->hash_mask}; }
 
 // Coordinate of the cell with linear id L along dimension lane_id() for the
 // lanes below k: the warp pays one 64-bit division per lane, and the other
@@ -104,32 +108,38 @@ __device__ __forceinline__ uint32_t div_w(uint32_t r, uint32_t w) {
     return w == 3u ? (uint32_t)(((unsigned long long)r * 0xAAAAAAABull) >> 33) : (w == 2u ? r >> 1 : r);
 }
 
-// Cell index of linear id `lid`, or kNoCell.  Probes stop at a free slot; the
-// table is at most half full, so the loop ends after a few probes (and after
-// capacity probes at the very most).
-__device__ __forceinline__ uint32_t cell_find(const HjCellHash& h, unsigned long long lid) {
-    unsigned long long i = mix64(lid) & h.mask;
+// The entry of group g: (first cell, id mask), or a zero mask when the group has
+// no cell.  Probes stop at a free entry; the table is at most half full, so the
+// loop ends after a few probes (and after capacity probes at the very most).
+__device__ __forceinline__ uint2 group_find(const HjCellHash& h, unsigned long long g) {
+    unsigned long long i = mix64(g) & h.mask;
     for (unsigned long long probe = 0; probe <= h.mask; ++probe) {
-        const unsigned long long key = h.keys[i];
-        if (key == lid) return h.vals[i];
-        if (key == kEmptyLid) return kNoCell;
+        const uint4 e = h.entries[i];
+        const unsigned long long key = ((unsigned long long)e.y << 32) | e.x;
+        if (key == g) return make_uint2(e.z, e.w);
+        if (key == kEmptyLid) break;
         i = (i + 1) & h.mask;
     }
-    return kNoCell;
+    return make_uint2(kNoCell, 0u);
 }
 
 // Points of the existing cells with linear ids lo .. lo + w - 1 (consecutive
-// along dimension 0): one contiguous span [x, y) of the cell-ordered points,
-// because the non-empty cells are sorted by linear id.
+// along dimension 0, w <= 4): one contiguous span [x, y) of the cell-ordered
+// points, because the non-empty cells are sorted by linear id.
 __device__ __forceinline__ uint2 cell_span(const HjCellHash& h, const uint32_t* cell_start, unsigned long long lo,
                                            uint32_t w) {
+    const unsigned long long hi = lo + w - 1;
     uint32_t first = kNoCell, last = kNoCell;
-    for (uint32_t i = 0; i < w; ++i) {
-        const uint32_t c = cell_find(h, lo + i);
-        if (c != kNoCell) {
-            if (first == kNoCell) first = c;
-            last = c;
-        }
+    for (unsigned long long g = lo >> 2; g <= (hi >> 2); ++g) {
+        const uint2 e = group_find(h, g);
+        const uint32_t b0 = g == (lo >> 2) ? (uint32_t)(lo & 3u) : 0u;
+        const uint32_t b1 = g == (hi >> 2) ? (uint32_t)(hi & 3u) : 3u;
+        const uint32_t m = e.y & ((2u << b1) - 1u) & ~((1u << b0) - 1u);   // the group's ids in [lo, hi]
+        if (m == 0u) continue;
+        const uint32_t f = e.x + __popc(e.y & ((1u << (__ffs(m) - 1)) - 1u));
+        const uint32_t l = e.x + __popc(e.y & ((2u << (31 - __clz(m))) - 1u)) - 1u;
+        if (first == kNoCell) first = f;
+        last = l;
     }
     if (first == kNoCell) return make_uint2(0u, 0u);
     return make_uint2(cell_start[first], cell_start[last + 1]);
