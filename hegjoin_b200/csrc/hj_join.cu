@@ -121,6 +121,8 @@ __global__ void k_batch_cuts(const double* __restrict__ pre, uint32_t nblocks, d
 // cells and probe the same hash slots, then run far apart and miss in L2.  In
 // cell (linear id) order consecutive light items share most of their stencil.
 constexpr uint32_t kLightCandidates = 4096;
+// Only lists this long are reordered: a small join saves the host round trip.
+constexpr uint32_t kLightMinItems = 65536;
 
 // Items whose cells have more candidates than `lim`: a prefix, since the items
 // follow the workload order (candidates non-increasing).
@@ -170,39 +172,114 @@ __global__ void k_batch_reset(JoinCtl* c) {
 // Grouping a batch's pairs by query id: a counting sort.  Keys are query ids
 // below n (sentinel slots are skipped), so one pass counts the pairs per query,
 // an exclusive scan over the n + 1 counters gives every query's first slot, and
-// one more pass scatters each pair to its query's run.  Lanes of a warp holding
-// the same key share one atomic (a leader adds the group's size).  Within a
-// query the order of its pairs is not defined, as in the reference (whose key
-// sort is unstable).
-__global__ void k_group_count(const uint32_t* __restrict__ keys, unsigned long long m, uint32_t* __restrict__ cnt) {
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
-         base += stride) {
-        const unsigned long long i = base + lane_id();
-        const uint32_t key = i < m ? keys[i] : kSentinelKey;
-        const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        if (key != kSentinelKey && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&cnt[key], __popc(peers));
+// one more pass scatters each pair to its query's run.  Within a query the order
+// of its pairs is not defined, as in the reference (whose key sort is unstable).
+//
+// Both passes work on tiles of 4,096 consecutive pairs per block.  A tile comes
+// mostly from one or two work items, so it holds a few dozen distinct queries:
+// the block gathers them in a shared-memory table (key -> slot, open addressing;
+// lanes of a warp with the same key share one table operation) and issues one
+// global atomic per query per tile instead of one per query per warp.  Keys
+// that find the table full take their global atomics directly.
+constexpr uint32_t kGrpPer = 16;                       // pairs per thread per tile
+constexpr uint32_t kGrpTile = 256 * kGrpPer;           // pairs per block-tile
+constexpr uint32_t kGrpSlots = 1024;                   // table slots (power of two)
+constexpr uint32_t kGrpFull = 0xFFFFFFFFu;
+
+// Slot of `key` in the block's table (inserting it), or kGrpFull.
+__device__ __forceinline__ uint32_t grp_slot(uint32_t* hk, uint32_t key) {
+    uint32_t h = (uint32_t)mix64(key) & (kGrpSlots - 1);
+    for (uint32_t probe = 0; probe < 64; ++probe) {
+        const uint32_t prev = atomicCAS(&hk[h], kSentinelKey, key);
+        if (prev == kSentinelKey || prev == key) return h;
+        h = (h + 1) & (kGrpSlots - 1);
+    }
+    return kGrpFull;
+}
+
+__global__ void __launch_bounds__(256) k_group_count(const uint32_t* __restrict__ keys, unsigned long long m,
+                                                      uint32_t* __restrict__ cnt) {
+    __shared__ uint32_t hk[kGrpSlots], hc[kGrpSlots];
+    for (unsigned long long base = (unsigned long long)blockIdx.x * kGrpTile; base < m;
+         base += (unsigned long long)gridDim.x * kGrpTile) {
+        for (uint32_t s = threadIdx.x; s < kGrpSlots; s += blockDim.x) { hk[s] = kSentinelKey; hc[s] = 0; }
+        __syncthreads();
+#pragma unroll 4
+        for (uint32_t j = 0; j < kGrpPer; ++j) {
+            const unsigned long long i = base + j * 256ull + threadIdx.x;
+            const uint32_t key = i < m ? keys[i] : kSentinelKey;
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            if (key != kSentinelKey && lane_id() == (uint32_t)(__ffs(peers) - 1)) {
+                const uint32_t sl = grp_slot(hk, key);
+                if (sl == kGrpFull) atomicAdd(&cnt[key], __popc(peers));
+                else atomicAdd(&hc[sl], __popc(peers));
+            }
+        }
+        __syncthreads();
+        for (uint32_t s = threadIdx.x; s < kGrpSlots; s += blockDim.x)
+            if (hk[s] != kSentinelKey) atomicAdd(&cnt[hk[s]], hc[s]);
+        __syncthreads();
     }
 }
 
-__global__ void k_group_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                                unsigned long long m, uint32_t* __restrict__ cursor, uint32_t* __restrict__ keys_out,
-                                uint32_t* __restrict__ vals_out) {
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
-         base += stride) {
-        const unsigned long long i = base + lane_id();
-        const uint32_t key = i < m ? keys[i] : kSentinelKey;
-        const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        const uint32_t leader = __ffs(peers) - 1;
-        uint32_t first = 0;
-        if (key != kSentinelKey && lane_id() == leader) first = atomicAdd(&cursor[key], __popc(peers));
-        first = __shfl_sync(0xffffffffu, first, leader);
-        if (key != kSentinelKey) {
-            const uint32_t pos = first + __popc(peers & lanemask_lt());
-            keys_out[pos] = key;
-            vals_out[pos] = vals[i];
+__global__ void __launch_bounds__(256) k_group_scatter(const uint32_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ vals, unsigned long long m,
+                                                        uint32_t* __restrict__ cursor, uint32_t* __restrict__ keys_out,
+                                                        uint32_t* __restrict__ vals_out) {
+    __shared__ uint32_t hk[kGrpSlots], hc[kGrpSlots];
+    for (unsigned long long base = (unsigned long long)blockIdx.x * kGrpTile; base < m;
+         base += (unsigned long long)gridDim.x * kGrpTile) {
+        for (uint32_t s = threadIdx.x; s < kGrpSlots; s += blockDim.x) { hk[s] = kSentinelKey; hc[s] = 0; }
+        __syncthreads();
+        // pass 1: the tile's pairs per query (the thread keeps its keys and values)
+        uint32_t kk[kGrpPer], vv[kGrpPer];
+#pragma unroll
+        for (uint32_t j = 0; j < kGrpPer; ++j) {
+            const unsigned long long i = base + j * 256ull + threadIdx.x;
+            kk[j] = i < m ? keys[i] : kSentinelKey;
+            vv[j] = i < m ? vals[i] : 0u;
         }
+#pragma unroll
+        for (uint32_t j = 0; j < kGrpPer; ++j) {
+            const uint32_t key = kk[j];
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            if (key != kSentinelKey && lane_id() == (uint32_t)(__ffs(peers) - 1)) {
+                const uint32_t sl = grp_slot(hk, key);
+                if (sl != kGrpFull) atomicAdd(&hc[sl], __popc(peers));
+            }
+        }
+        __syncthreads();
+        // one global reservation per query of the tile; the slot's count becomes its cursor
+        for (uint32_t s = threadIdx.x; s < kGrpSlots; s += blockDim.x)
+            if (hk[s] != kSentinelKey) hc[s] = atomicAdd(&cursor[hk[s]], hc[s]);
+        __syncthreads();
+        // pass 2: place the pairs
+#pragma unroll
+        for (uint32_t j = 0; j < kGrpPer; ++j) {
+            const uint32_t key = kk[j];
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            const uint32_t leader = __ffs(peers) - 1;
+            uint32_t first = 0;
+            if (key != kSentinelKey && lane_id() == leader) {
+                uint32_t sl = kGrpFull;
+                // the key is in the table unless the table was full when it came
+                uint32_t h = (uint32_t)mix64(key) & (kGrpSlots - 1);
+                for (uint32_t probe = 0; probe < 64; ++probe) {
+                    const uint32_t k2 = hk[h];
+                    if (k2 == key) { sl = h; break; }
+                    if (k2 == kSentinelKey) break;
+                    h = (h + 1) & (kGrpSlots - 1);
+                }
+                first = sl != kGrpFull ? atomicAdd(&hc[sl], __popc(peers)) : atomicAdd(&cursor[key], __popc(peers));
+            }
+            first = __shfl_sync(0xffffffffu, first, leader);
+            if (key != kSentinelKey) {
+                const uint32_t pos = first + __popc(peers & lanemask_lt());
+                keys_out[pos] = key;
+                vals_out[pos] = vv[j];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -545,7 +622,7 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     uint32_t nblocks = 0;
     HJ_TRY(build_blocks(ix, qb, &blocks, &nblocks, st));
     tmp.adopt(blocks);
-    if (!tc && nblocks > 1) {
+    if (!tc && nblocks >= kLightMinItems) {
         // the light items' tail in cell order (kLightCandidates)
         unsigned int* dh = nullptr;
         HJ_TRY(tmp.alloc(&dh, 1));
@@ -873,7 +950,7 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
         if (slots) {
             // group by query id: count, scan (qoff[n] = the batch's pairs), scatter into the copies
             HJ_CUDA(cudaMemsetAsync(qoff, 0, ((size_t)ix->n + 1) * 4, st));
-            const unsigned g = (unsigned)std::min<uint64_t>((slots + 255) / 256, (uint64_t)num_sms() * 16);
+            const unsigned g = (unsigned)std::min<uint64_t>((slots + kGrpTile - 1) / kGrpTile, (uint64_t)num_sms() * 8);
             k_group_count<<<g, 256, 0, st>>>(keys, slots, qoff);
             HJ_LAUNCHED();
             HJ_TRY(scan_u32_inplace(qoff, (uint64_t)ix->n + 1, st));
