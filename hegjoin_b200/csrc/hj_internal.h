@@ -68,6 +68,7 @@ struct hj_index {
     float* tc_err = nullptr;         // per sorted point: quantisation error norm (rounded up)
     float* tc_pband = nullptr;       // per sorted point: its part of the guard band (rounded up)
     uint32_t tc_kpad = 0;
+    int plain_shape = 0;             // exact refine tile shape (0 or 1; autotuned per d and dtype)
     int tc_kind = -1;                // HJ_REFINE_TC_F16 / _BF16 the operands hold
     void* tc_state = nullptr;        // tensor maps and error maxima (hj_refine_tc.cu)
 };

@@ -785,8 +785,34 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             }
             tc_set_epi(ix, best_epi);
             tune_store(key, best_epi);
+        } else if (!tc && nsamp >= 16 && !tune_lookup(key, &tuned) && tuning_enabled()) {
+            // the exact refine's two tile shapes, timed on the sample (each run twice, the
+            // faster run kept: the first run of a shape also pays its one-time setup); the
+            // last run's counts are the estimate, and they are the same for either shape
+            float best = 1e30f;
+            int best_shape = 0;
+            EventPairs tev;
+            tev.ev.emplace_back(nullptr, nullptr);
+            HJ_TRY(event_acquire(&tev.ev[0].first));
+            HJ_TRY(event_acquire(&tev.ev[0].second));
+            for (int shape : {1, 0}) {
+                ix->plain_shape = shape;
+                for (int rep = 0; rep < 2; ++rep) {
+                    HJ_CUDA(cudaMemsetAsync(scnt, 0, nsamp * sizeof(unsigned long long), st));
+                    HJ_CUDA(cudaEventRecord(tev.ev[0].first, st));
+                    HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
+                    HJ_CUDA(cudaEventRecord(tev.ev[0].second, st));
+                    HJ_CUDA(cudaEventSynchronize(tev.ev[0].second));
+                    float ms = 0;
+                    HJ_CUDA(cudaEventElapsedTime(&ms, tev.ev[0].first, tev.ev[0].second));
+                    if (ms < best) { best = ms; best_shape = shape; }
+                }
+            }
+            ix->plain_shape = best_shape;   // the exact counts of the last run do not depend on the shape
+            tune_store(key, best_shape);
         } else {
             if (tc && tuned) tc_set_epi(ix, tuned);
+            if (!tc) ix->plain_shape = tuned;
             HJ_TRY(run_refine(sblocks, nsamp, none, no_band, 1, scnt));
             HJ_TRY(check_timeout());
         }

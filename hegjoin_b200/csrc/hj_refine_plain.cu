@@ -440,28 +440,41 @@ hj_status launch_t(const PlainArgs<T>& args, cudaStream_t st) {
     return HJ_OK;
 }
 
+// Two tile shapes per dimension class, both with 64-query work items and 256
+// threads: 64 queries x 128 candidates per staged chunk (4 x 8 per thread) and
+// 64 x 64 (4 x 4 per thread).  The wide one stages half as many chunks (half
+// the barriers) but holds twice the accumulators; which wins depends on d, the
+// type and the hit density, so the join times both on the estimator's sample
+// (shape 0 is each type's default: wide for float, narrow for double).
+template <typename T, int D>
+hj_status launch_shape(const PlainArgs<T>& a, int wide, cudaStream_t st) {
+    return wide ? launch_t<T, D, 64, 128, 4, 8>(a, st) : launch_t<T, D, 64, 64, 4, 4>(a, st);
+}
+
 template <typename T>
-hj_status dispatch_t(const PlainArgs<T>& args, cudaStream_t st);
+hj_status dispatch_t(const PlainArgs<T>& args, int shape, cudaStream_t st);
 
 template <>
-hj_status dispatch_t<float>(const PlainArgs<float>& a, cudaStream_t st) {
+hj_status dispatch_t<float>(const PlainArgs<float>& a, int shape, cudaStream_t st) {
+    const int wide = shape == 0;
     switch (a.d) {
-        case 2: return launch_t<float, 2, 64, 128, 4, 8>(a, st);
-        case 3: return launch_t<float, 3, 64, 128, 4, 8>(a, st);
-        case 6: return launch_t<float, 6, 64, 128, 4, 8>(a, st);
-        case 18: return launch_t<float, 18, 64, 128, 4, 8>(a, st);
-        case 32: return launch_t<float, 32, 64, 128, 4, 8>(a, st);
-        case 90: return launch_t<float, 90, 64, 128, 4, 8>(a, st);
-        default: return launch_t<float, 0, 64, 128, 4, 8>(a, st);
+        case 2: return launch_shape<float, 2>(a, wide, st);
+        case 3: return launch_shape<float, 3>(a, wide, st);
+        case 6: return launch_shape<float, 6>(a, wide, st);
+        case 18: return launch_shape<float, 18>(a, wide, st);
+        case 32: return launch_shape<float, 32>(a, wide, st);
+        case 90: return launch_shape<float, 90>(a, wide, st);
+        default: return launch_shape<float, 0>(a, wide, st);
     }
 }
 template <>
-hj_status dispatch_t<double>(const PlainArgs<double>& a, cudaStream_t st) {
+hj_status dispatch_t<double>(const PlainArgs<double>& a, int shape, cudaStream_t st) {
+    const int wide = shape != 0;
     switch (a.d) {
-        case 2: return launch_t<double, 2, 64, 64, 4, 4>(a, st);
-        case 3: return launch_t<double, 3, 64, 64, 4, 4>(a, st);
-        case 6: return launch_t<double, 6, 64, 64, 4, 4>(a, st);
-        default: return launch_t<double, 0, 64, 64, 4, 4>(a, st);
+        case 2: return launch_shape<double, 2>(a, wide, st);
+        case 3: return launch_shape<double, 3>(a, wide, st);
+        case 6: return launch_shape<double, 6>(a, wide, st);
+        default: return launch_shape<double, 0>(a, wide, st);
     }
 }
 
@@ -486,12 +499,12 @@ hj_status launch_refine_plain(const hj_index* ix, const HjBlock* blocks, uint32_
         PlainArgs<float> a{(const float*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, cell_hash(ix), ix->d,
                            ix->grid,
                            (float)ix->thr, blocks, nblocks, head, sink, count_only, block_counts};
-        return dispatch_t<float>(a, st);
+        return dispatch_t<float>(a, ix->plain_shape, st);
     }
     PlainArgs<double> a{(const double*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, cell_hash(ix), ix->d,
                         ix->grid,
                         ix->thr, blocks, nblocks, head, sink, count_only, block_counts};
-    return dispatch_t<double>(a, st);
+    return dispatch_t<double>(a, ix->plain_shape, st);
 }
 
 }  // namespace hj
