@@ -59,7 +59,8 @@ class JoinOpts(ctypes.Structure):
     _fields_ = [("refine", ctypes.c_int), ("result_capacity", ctypes.c_uint64), ("sample_rate", ctypes.c_double),
                 ("mem_fraction", ctypes.c_double), ("query_block", ctypes.c_uint32), ("max_batches", ctypes.c_uint32),
                 ("use_graphs", ctypes.c_uint32), ("keep_keys", ctypes.c_uint32), ("shard_count", ctypes.c_uint32),
-                ("shard_index", ctypes.c_uint32), ("device_bytes_cap", ctypes.c_uint64)]
+                ("shard_index", ctypes.c_uint32), ("device_bytes_cap", ctypes.c_uint64),
+                ("stream_overlap", ctypes.c_uint32)]
 
 
 class JoinStats(ctypes.Structure):
@@ -76,7 +77,7 @@ class JoinStats(ctypes.Structure):
 
 class BatchView(ctypes.Structure):
     _fields_ = [("batch", ctypes.c_uint32), ("pad_", ctypes.c_uint32), ("count", ctypes.c_uint64),
-                ("d_keys", ctypes.c_void_p), ("d_vals", ctypes.c_void_p)]
+                ("d_keys", ctypes.c_void_p), ("d_vals", ctypes.c_void_p), ("release_event", ctypes.c_void_p)]
 
 
 # hj_batch_sink: hj_status (*)(const hj_batch_view*, void* user, void* stream)
@@ -336,7 +337,8 @@ class JoinResult:
 
 
 def join_opts(refine="auto", result_capacity=0, sample_rate=0.0, mem_fraction=0.0, max_batches=0,
-              use_graphs=False, keep_keys=False, shard_count=0, shard_index=0, device_bytes_cap=0) -> JoinOpts:
+              use_graphs=False, keep_keys=False, shard_count=0, shard_index=0, device_bytes_cap=0,
+              stream_overlap=False) -> JoinOpts:
     o = JoinOpts()
     lib.hj_join_opts_default(ctypes.byref(o))
     o.refine = REFINE_NAMES[refine] if isinstance(refine, str) else int(refine)
@@ -351,6 +353,7 @@ def join_opts(refine="auto", result_capacity=0, sample_rate=0.0, mem_fraction=0.
     o.shard_count = int(shard_count)
     o.shard_index = int(shard_index)
     o.device_bytes_cap = int(device_bytes_cap)
+    o.stream_overlap = int(bool(stream_overlap))
     return o
 
 
@@ -371,7 +374,10 @@ def join_stream(index: GridIndex, sink=None, digest: bool = True, stream=None, *
     """The join with nothing kept on the device (hj_join_stream): every grouped batch
     goes to `sink(batch, count, keys_ptr, vals_ptr, stream_ptr)` (device pointers,
     valid for work enqueued on that stream) and per-query digests accumulate on the
-    device.  Returns (JoinStats, (count, sum, xor) CUDA tensors or None)."""
+    device.  With stream_overlap=True the sink may instead read the batch on a stream
+    of its own and return (status, event_handle): a raw cudaEvent_t recorded after
+    those reads (e.g. torch.cuda.Event().cuda_event), kept alive until the join
+    returns.  Returns (JoinStats, (count, sum, xor) CUDA tensors or None)."""
     torch = _torch()
     n = index.info().n
     dev = index.db.device
@@ -386,6 +392,9 @@ def join_stream(index: GridIndex, sink=None, digest: bool = True, stream=None, *
         try:
             v = view.contents
             r = sink(int(v.batch), int(v.count), v.d_keys, v.d_vals, st)
+            if isinstance(r, tuple):
+                r, ev = r
+                view.contents.release_event = ev
             return HJ_OK if r is None else int(r)
         except Exception as e:          # a Python error stops the join with a clear status
             errors.append(e)

@@ -567,6 +567,10 @@ struct BatchHandler {
     // valid in the order of `st` until the next batch's refine is enqueued.
     virtual hj_status on_batch(uint32_t batch, const uint32_t* keys, const uint32_t* vals, uint64_t count,
                                cudaStream_t st) = 0;
+    // Whether the handler can use two alternating sets of grouped arrays, and the event
+    // (if any) after which the last batch's set may be reused.
+    virtual bool can_overlap() const { return false; }
+    virtual cudaEvent_t take_release() { return nullptr; }
 };
 
 // The batched join (distanceTableNDGridBatches, GPU.cu:787-1702): refine kind,
@@ -840,7 +844,10 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     // slack for partly filled warp chunks: every warp that can emit during a batch holds
     // at most one (sized from the launch grids, so small joins get small buffers)
     const uint64_t chunk_slack = (tc ? tc_emit_warps(nblocks) : plain_emit_warps(nblocks)) * kSinkChunk;
-    const uint32_t slot_words = tc ? 6u : 4u;   // keys, vals, their radix copies (+ band pair ids)
+    // keys, vals, their grouped copies (+ band pair ids; + a second set of grouped copies)
+    const bool overlap = opts.stream_overlap && handler.can_overlap();
+    const uint32_t base_words = tc ? 6u : 4u;
+    const uint32_t slot_words = base_words + (overlap ? 2u : 0u);
     const double bytes_per_slot = 4.0 * slot_words;
     const uint64_t want = (uint64_t)(total_est * 2.0) + chunk_slack + 4096;
     uint64_t cap = opts.result_capacity ? opts.result_capacity + chunk_slack : want;
@@ -929,6 +936,10 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     uint32_t *keys = slab, *vals = slab + cap, *keys_tmp = slab + 2 * cap, *vals_tmp = slab + 3 * cap;
     uint32_t* band_q = tc ? slab + 4 * cap : nullptr;
     uint32_t* band_c = tc ? slab + 5 * cap : nullptr;
+    // the grouped copies, one set per batch parity with stream_overlap
+    uint32_t* grp_keys[2] = {keys_tmp, overlap ? slab + (size_t)base_words * cap : keys_tmp};
+    uint32_t* grp_vals[2] = {vals_tmp, overlap ? slab + (size_t)(base_words + 1) * cap : vals_tmp};
+    cudaEvent_t release[2] = {nullptr, nullptr};   // a sink's events: the set is still being read
     uint32_t* qoff = nullptr;   // per-query counters, then first slots, of the grouping
     HJ_TRY(tmp.alloc(&qoff, (size_t)ix->n + 1));
 
@@ -981,7 +992,12 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             HJ_LAUNCHED();
             HJ_TRY(scan_u32_inplace(qoff, (uint64_t)ix->n + 1, st));
             HJ_CUDA(cudaMemcpyAsync(&valid, qoff + ix->n, 4, cudaMemcpyDeviceToHost, st));
-            k_group_scatter<<<g, 256, 0, st>>>(keys, vals, slots, qoff, keys_tmp, vals_tmp);
+            const int set = overlap ? (int)(n_out & 1u) : 0;
+            if (release[set]) {   // the sink's reads of this set, two batches ago
+                HJ_CUDA(cudaStreamWaitEvent(st, release[set], 0));
+                release[set] = nullptr;
+            }
+            k_group_scatter<<<g, 256, 0, st>>>(keys, vals, slots, qoff, grp_keys[set], grp_vals[set]);
             HJ_LAUNCHED();
             HJ_CUDA(cudaStreamSynchronize(st));
         }
@@ -1000,11 +1016,21 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             return HJ_ERR_OOM;
         }
         kept += kept_bytes_per_pair * (double)valid;
-        HJ_TRY(handler.on_batch(n_out, keys_tmp, vals_tmp, valid, st));
+        {
+            const int set = overlap ? (int)(n_out & 1u) : 0;
+            if (release[set]) {   // an empty batch reuses the set without a scatter
+                HJ_CUDA(cudaStreamWaitEvent(st, release[set], 0));
+                release[set] = nullptr;
+            }
+            HJ_TRY(handler.on_batch(n_out, grp_keys[set], grp_vals[set], valid, st));
+            release[set] = handler.take_release();
+        }
         ++n_out;
         total += valid;
         ms_group += ms_since(t_g);
     }
+    for (cudaEvent_t e : release)
+        if (e) HJ_CUDA(cudaStreamWaitEvent(st, e, 0));   // the sink's last reads end before the join does
     HJ_CUDA(cudaStreamSynchronize(st));
     S.ms_refine = ms_since(t_ref) - ms_group;
     S.ms_group = ms_group;
@@ -1077,14 +1103,22 @@ struct StreamHandler : BatchHandler {
             HJ_LAUNCHED();
         }
         if (!sink) return HJ_OK;
-        hj_batch_view v{bi, 0u, count, keys, vals};
+        hj_batch_view v{bi, 0u, count, keys, vals, nullptr};
         hj_status s = sink(&v, user, st);
+        last_release = static_cast<cudaEvent_t>(v.release_event);
         if (s != HJ_OK) {
             set_error("hj_join_stream: the batch sink returned %d", s);
             return s;
         }
         return HJ_OK;
     }
+    bool can_overlap() const override { return sink != nullptr; }
+    cudaEvent_t take_release() override {
+        cudaEvent_t e = last_release;
+        last_release = nullptr;
+        return e;
+    }
+    cudaEvent_t last_release = nullptr;
 };
 
 }  // namespace

@@ -105,6 +105,10 @@ typedef struct {
                                       join keeps (hj_join: neighbour ids and table); 0 = none.  A join
                                       that cannot fit returns HJ_ERR_OOM with stats->bytes_wanted set,
                                       before its results would pass the cap */
+    uint32_t stream_overlap;       /* hj_join_stream: grouped batches alternate between two sets of
+                                      arrays, so a sink may read a batch on a stream of its own while
+                                      the next batches run (see hj_batch_view.release_event); costs two
+                                      more words of device memory per result slot.  0 = one set */
 } hj_join_opts;
 
 typedef struct {
@@ -239,11 +243,18 @@ typedef struct {
     uint64_t count;
     const uint32_t* d_keys;
     const uint32_t* d_vals;
+    void* release_event;           /* set by the sink (optional, with stream_overlap): a cudaEvent_t
+                                      recorded after its last use of d_keys / d_vals; NULL on entry */
 } hj_batch_view;
 /* Called on the joining thread once per batch.  The arrays stay valid for work
  * the sink enqueues on `stream` (copies, kernels): the next batch reuses them
- * only after that work, in stream order.  Return HJ_OK to continue; any other
- * status stops the join and is returned by hj_join_stream. */
+ * only after that work, in stream order.  With hj_join_opts.stream_overlap the
+ * arrays are not touched again until two batches later, and a sink may instead
+ * use them from a stream of its own (after waiting for an event it records on
+ * `stream`) and hand back, in release_event, an event recorded after that use:
+ * the join waits for it before it reuses the arrays and before it returns.
+ * The event must stay valid until hj_join_stream returns.  Return HJ_OK to
+ * continue; any other status stops the join and is returned by hj_join_stream. */
 typedef hj_status (*hj_batch_sink)(const hj_batch_view* batch, void* user, void* stream);
 
 /* The join of hj_join with nothing kept on the device: each batch is grouped by

@@ -81,3 +81,47 @@ def test_stream_without_sink_and_sink_error(cuda):
     assert e.value.status == hj.HJ_ERR_CUDA and "sink" in str(e.value)
     torch.cuda.synchronize()
     assert hj.debug_pool_used() == base
+
+
+@pytest.mark.parametrize("refine", ["exact", "auto"])
+def test_stream_overlap_sink_on_its_own_stream(cuda, refine):
+    """With stream_overlap, a sink that reads each batch on a stream of its own (after
+    waiting for the batch on the join's stream) and hands back an event gets every batch
+    intact, although the next batches run meanwhile."""
+    import torch
+    import hegjoin_b200 as hj
+    d, k, eps, dtype = (2, 2, 0.01, np.float64) if refine == "exact" else (18, 6, 0.09, np.float32)
+    db = workloads.exp40(82, 20000, d, dtype)
+    ix, mn, nc = _index(db, k, eps, cuda)
+    off, vals = oracle.join(db, k, eps, mn, nc)
+    total = int(off[-1])
+    side = torch.cuda.Stream()
+    keep, events = [], []
+
+    def sink(batch, count, keys, vals_p, stream):
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.ExternalStream(stream) if stream else torch.cuda.default_stream())
+        side.wait_event(ready)
+        with torch.cuda.stream(side):
+            # a slow reader: copies made on the side stream, after some unrelated work
+            pad = torch.ones(1 << 22, device=cuda)
+            for _ in range(20):
+                pad = pad * 1.0001
+            if count:
+                keep.append((hj.device_view(keys, (count,), np.uint32).clone(),
+                             hj.device_view(vals_p, (count,), np.uint32).clone()))
+        done = torch.cuda.Event()
+        done.record(side)
+        events.append((ready, done, pad))
+        return 0, done.cuda_event
+
+    st, _ = hj.join_stream(ix, sink, refine=refine, result_capacity=max(1, total // 7), stream_overlap=True)
+    torch.cuda.synchronize()
+    assert st.total_pairs == total and st.n_batches > 2
+    keys = np.concatenate([a.cpu().numpy() for a, _ in keep])
+    v = np.concatenate([b.cpu().numpy() for _, b in keep])
+    order = np.lexsort((v, keys))
+    keys, v = keys[order], v[order]
+    goff = np.zeros(len(db) + 1, np.uint64)
+    np.cumsum(np.bincount(keys, minlength=len(db)), out=goff[1:])
+    assert np.array_equal(goff, off) and np.array_equal(v, vals)
