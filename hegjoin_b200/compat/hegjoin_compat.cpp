@@ -186,7 +186,7 @@ void distanceTableNDGridBatches(int searchMode, float staticPartition, unsigned 
             if (keys) cudaFreeHost(keys);
             if (vals) cudaFreeHost(vals);
         }
-        static hj_status on_batch(const hj_batch_view* b, void* user, void* stream) {
+        static hj_status on_batch(hj_batch_view* b, void* user, void* stream) {
             Sink* S = static_cast<Sink*>(user);
             if (b->count == 0) return HJ_OK;
             if (b->count > 0x7FFFFFFFull) return HJ_ERR_OVERFLOW;   // the table stores int offsets

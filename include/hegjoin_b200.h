@@ -255,7 +255,7 @@ typedef struct {
  * the join waits for it before it reuses the arrays and before it returns.
  * The event must stay valid until hj_join_stream returns.  Return HJ_OK to
  * continue; any other status stops the join and is returned by hj_join_stream. */
-typedef hj_status (*hj_batch_sink)(const hj_batch_view* batch, void* user, void* stream);
+typedef hj_status (*hj_batch_sink)(hj_batch_view* batch, void* user, void* stream);
 
 /* The join of hj_join with nothing kept on the device: each batch is grouped by
  * query id and handed to `sink` (may be NULL), and its buffers are reused by
