@@ -421,15 +421,6 @@ hj_status index_create_t(const T* d_db, uint32_t n, uint32_t d, uint32_t k, T ep
     return HJ_OK;
 }
 
-// Cells that open a group (the first of their lid >> 2): their number, for the
-// capacity.
-__global__ void k_count_groups(const unsigned long long* __restrict__ lid, uint32_t nC, unsigned int* groups) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool opens = i < nC && (i == 0 || (lid[i - 1] >> 2) != (lid[i] >> 2));
-    const uint32_t c = __popc(__ballot_sync(0xffffffffu, opens));
-    if (lane_id() == 0 && c) atomicAdd(groups, c);
-}
-
 // The first cell of each group inserts the group's entry: key, first cell, mask
 // of the group's ids (its cells are the next ones in the table, at most four).
 // The key word pair is claimed with a 64-bit compare-and-swap on the entry's
@@ -456,23 +447,11 @@ __global__ void k_hash_insert(const unsigned long long* __restrict__ lid, uint32
 }
 
 // The cell hash of an index whose cell table is built (capacity: the power of
-// two at least twice the number of groups, at least 64).
+// two at least twice the number of cells, an upper bound on the groups that
+// needs no count from the device, at least 64).
 hj_status build_cell_hash(hj_index* ix, cudaStream_t st) {
-    unsigned long long groups = 0;
-    if (ix->nC) {
-        Scratch tmp(st);
-        unsigned int* dg = nullptr;
-        HJ_TRY(tmp.alloc(&dg, 1));
-        HJ_CUDA(cudaMemsetAsync(dg, 0, sizeof(unsigned int), st));
-        k_count_groups<<<(ix->nC + 255) / 256, 256, 0, st>>>(ix->cell_lid, ix->nC, dg);
-        HJ_LAUNCHED();
-        unsigned int hg = 0;
-        HJ_CUDA(cudaMemcpyAsync(&hg, dg, sizeof(hg), cudaMemcpyDeviceToHost, st));
-        HJ_CUDA(cudaStreamSynchronize(st));
-        groups = hg;
-    }
     unsigned long long cap = 64;
-    while (cap < 2ull * groups) cap <<= 1;
+    while (cap < 2ull * ix->nC) cap <<= 1;
     HJ_TRY(dalloc(&ix->hash_entries, (size_t)cap, st));
     HJ_CUDA(cudaMemsetAsync(ix->hash_entries, 0xFF, (size_t)cap * sizeof(uint4), st));
     ix->hash_mask = cap - 1;

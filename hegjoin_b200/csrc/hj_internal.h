@@ -18,7 +18,8 @@ struct HjGrid {
 // plus the number of mask bits below b.  A stencil row (up to 3 consecutive ids
 // along dimension 0) spans one or two groups: one or two 16-byte loads, and
 // neighbouring cells along dimension 0 hit the same entries.  Capacity is a
-// power of two at least twice the number of groups; free entries hold the key
+// power of two at least twice the number of cells (so at most half full of
+// groups); free entries hold the key
 // kEmptyLid (no group can have it: linear ids stay below 2^63).
 struct HjCellHash {
     const uint4* entries;
