@@ -35,9 +35,10 @@
 
 namespace hj {
 uint32_t plain_query_block(int dtype);
+bool plain_counts_queries(const hj_index* ix);
 hj_status launch_refine_plain(const hj_index* ix, const HjBlock* blocks, uint32_t nblocks, unsigned int* head,
                               const PairSink& sink, uint32_t count_only, unsigned long long* block_counts,
-                              cudaStream_t st);
+                              uint32_t* qcount, cudaStream_t st);
 hj_status tc_prepare(hj_index* ix, int kind, cudaStream_t st);
 uint32_t tc_query_block();
 hj_status launch_refine_tc(const hj_index* ix, const HjBlock* blocks, uint32_t nblocks, unsigned int* head,
@@ -701,7 +702,8 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     EventPairs kev;   // refine kernel launches of the join proper
     // head_reset: zero the work-item queue head first (batches reset it with the rest)
     auto run_refine = [&](const HjBlock* blk, uint32_t nb, const PairSink& sink, const PairSink& band,
-                          uint32_t count_only, unsigned long long* bc, bool head_reset = true) -> hj_status {
+                          uint32_t count_only, unsigned long long* bc, bool head_reset = true,
+                          uint32_t* qcount = nullptr) -> hj_status {
         if (head_reset) HJ_CUDA(cudaMemsetAsync(head, 0, sizeof(unsigned int), st));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (!count_only) {
@@ -714,7 +716,7 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
         }
         HJ_TRY(tc ? launch_refine_tc(ix, blk, nb, head, sink, band, count_only, bc,
                                      count_only ? nullptr : &ctl->tc_acc, &ctl->timeout, st)
-                  : launch_refine_plain(ix, blk, nb, head, sink, count_only, bc, st));
+                  : launch_refine_plain(ix, blk, nb, head, sink, count_only, bc, qcount, st));
         if (!count_only) HJ_CUDA(cudaEventRecord(e1, st));
         return HJ_OK;
     };
@@ -942,6 +944,9 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     cudaEvent_t release[2] = {nullptr, nullptr};   // a sink's events: the set is still being read
     uint32_t* qoff = nullptr;   // per-query counters, then first slots, of the grouping
     HJ_TRY(tmp.alloc(&qoff, (size_t)ix->n + 1));
+    // the exact refine counts each query's pairs itself when every item takes its block path
+    // (no warp path below k = 4): the grouping then skips its counting pass
+    const bool fused_counts = !tc && plain_counts_queries(ix);
 
     auto t_ref = std::chrono::steady_clock::now();
     float ms_group = 0;
@@ -959,7 +964,8 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
         HJ_LAUNCHED();
         PairSink sink{keys, vals, &ctl->cursor, cap, overflow};
         PairSink band = tc ? PairSink{band_q, band_c, &ctl->band_cursor, cap, overflow} : no_band;
-        HJ_TRY(run_refine(blocks + b.b0, b.b1 - b.b0, sink, band, 0, nullptr, false));
+        if (fused_counts) HJ_CUDA(cudaMemsetAsync(qoff, 0, ((size_t)ix->n + 1) * 4, st));
+        HJ_TRY(run_refine(blocks + b.b0, b.b1 - b.b0, sink, band, 0, nullptr, false, fused_counts ? qoff : nullptr));
         if (tc) HJ_TRY(launch_band_recheck(ix, band_q, band_c, &ctl->band_cursor, cap, sink, b.b1 - b.b0, st));
         JoinCtl hc;
         HJ_CUDA(cudaMemcpyAsync(&hc, ctl, sizeof(JoinCtl), cudaMemcpyDeviceToHost, st));
@@ -985,11 +991,14 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
         const uint64_t slots = std::min<uint64_t>(used, cap);
         uint32_t valid = 0;
         if (slots) {
-            // group by query id: count, scan (qoff[n] = the batch's pairs), scatter into the copies
-            HJ_CUDA(cudaMemsetAsync(qoff, 0, ((size_t)ix->n + 1) * 4, st));
+            // group by query id: count (unless the refine counted), scan (qoff[n] = the batch's
+            // pairs), scatter into the copies
             const unsigned g = (unsigned)std::min<uint64_t>((slots + kGrpTile - 1) / kGrpTile, (uint64_t)num_sms() * 8);
-            k_group_count<<<g, 256, 0, st>>>(keys, slots, qoff);
-            HJ_LAUNCHED();
+            if (!fused_counts) {
+                HJ_CUDA(cudaMemsetAsync(qoff, 0, ((size_t)ix->n + 1) * 4, st));
+                k_group_count<<<g, 256, 0, st>>>(keys, slots, qoff);
+                HJ_LAUNCHED();
+            }
             HJ_TRY(scan_u32_inplace(qoff, (uint64_t)ix->n + 1, st));
             HJ_CUDA(cudaMemcpyAsync(&valid, qoff + ix->n, 4, cudaMemcpyDeviceToHost, st));
             const int set = overlap ? (int)(n_out & 1u) : 0;

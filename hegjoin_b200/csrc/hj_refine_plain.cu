@@ -49,7 +49,16 @@ struct PlainArgs {
     PairSink sink;
     uint32_t count_only;
     unsigned long long* block_counts;   // count-only mode: pairs per work item
+    uint32_t* qcount;                   // optional: pairs per query (original id), written by the block
+                                        // path's items where plain_counts_queries() holds; zeroed by the caller
 };
+
+// Dimension classes whose refine counts each query's pairs (qcount): 2-D and 3-D,
+// the low dimensions where pairs far outnumber the arithmetic (the counters cost
+// registers that higher d needs).  Only without the warp path (k < 4) does every
+// item take the block path that counts.
+template <int D>
+constexpr bool kCountsQueries = D == 2 || D == 3;
 
 
 // Packed FP32 pairs (sm_100): each lane's result is the IEEE-rounded scalar
@@ -252,6 +261,9 @@ __global__ void __launch_bounds__(256, 3) k_refine_plain(PlainArgs<T> a) {
             if (j > 0) rows *= w[j];
         }
         unsigned long long item_cnt = 0;
+        uint32_t qc[RQ];   // this thread's pairs per query of its tile rows (qcount)
+#pragma unroll
+        for (int r = 0; r < RQ; ++r) qc[r] = 0;
         if (!empty) {
             for (uint32_t row0 = 0; row0 < rows; row0 += kRowGroup) {
                 const uint32_t nr = min(kRowGroup, rows - row0);
@@ -395,6 +407,12 @@ __global__ void __launch_bounds__(256, 3) k_refine_plain(PlainArgs<T> a) {
                     if (a.count_only) {
                         item_cnt += __popc(mask);
                     } else {
+                        if constexpr (kCountsQueries<D>) {
+                            if (a.qcount) {
+#pragma unroll
+                                for (int r = 0; r < RQ; ++r) qc[r] += __popc((mask >> (r * RC)) & ((1u << RC) - 1u));
+                            }
+                        }
                         // coalesced output: each lane writes every 32nd pair of the warp's hits
                         const uint32_t wbase = tid & ~31u;
                         warp_emit_masks(a.sink, wc, mask, [&](uint32_t owner, uint32_t b) {
@@ -410,6 +428,20 @@ __global__ void __launch_bounds__(256, 3) k_refine_plain(PlainArgs<T> a) {
         if (a.count_only) {
             for (int o = 16; o > 0; o >>= 1) item_cnt += __shfl_down_sync(0xffffffffu, item_cnt, o);
             if (lane_id() == 0 && item_cnt) atomicAdd(&a.block_counts[item], item_cnt);
+        } else if constexpr (kCountsQueries<D>) {
+            if (a.qcount) {
+                // the TX threads of a tile row share its RQ queries: sum over them, one store
+                // per query (a query belongs to one item of a batch)
+                static_assert(TX <= 32 && (32 % TX) == 0, "tile rows within a warp");
+#pragma unroll
+                for (int r = 0; r < RQ; ++r) {
+                    uint32_t v = qc[r];
+#pragma unroll
+                    for (int o = TX / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    const uint32_t qi = ty * RQ + r;
+                    if (tx == 0 && qi < nq && v) a.qcount[qid_s[qi]] = v;
+                }
+            }
         }
         __syncthreads();
     }
@@ -482,6 +514,10 @@ hj_status dispatch_t<double>(const PlainArgs<double>& a, int shape, cudaStream_t
 
 uint32_t plain_query_block(int dtype) { return 64; (void)dtype; }
 
+// Whether the exact refine writes each query's pair count (PlainArgs::qcount) for
+// this index: a counting dimension class, and every item on the block path.
+bool plain_counts_queries(const hj_index* ix) { return ix->grid.k < 4 && (ix->d == 2 || ix->d == 3); }
+
 // Upper bound on the warps of one refine launch that reserve pair-sink chunks (each
 // holds at most one partly filled chunk): at most 8 blocks of 8 warps per SM, and
 // never more blocks than work items.
@@ -493,17 +529,17 @@ uint64_t plain_emit_warps(uint32_t nblocks) {
 // zero on entry.  count_only: per-item pair counts go to block_counts.
 hj_status launch_refine_plain(const hj_index* ix, const HjBlock* blocks, uint32_t nblocks, unsigned int* head,
                               const PairSink& sink, uint32_t count_only, unsigned long long* block_counts,
-                              cudaStream_t st) {
+                              uint32_t* qcount, cudaStream_t st) {
     if (nblocks == 0) return HJ_OK;
     if (ix->dtype == HJ_F32) {
         PlainArgs<float> a{(const float*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, cell_hash(ix), ix->d,
                            ix->grid,
-                           (float)ix->thr, blocks, nblocks, head, sink, count_only, block_counts};
+                           (float)ix->thr, blocks, nblocks, head, sink, count_only, block_counts, qcount};
         return dispatch_t<float>(a, ix->plain_shape, st);
     }
     PlainArgs<double> a{(const double*)ix->pts, ix->perm, ix->cell_lid, ix->cell_start, ix->nC, cell_hash(ix), ix->d,
                         ix->grid,
-                        ix->thr, blocks, nblocks, head, sink, count_only, block_counts};
+                        ix->thr, blocks, nblocks, head, sink, count_only, block_counts, qcount};
     return dispatch_t<double>(a, ix->plain_shape, st);
 }
 
