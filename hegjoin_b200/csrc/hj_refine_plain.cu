@@ -85,16 +85,21 @@ __device__ __forceinline__ double ffma(double a, double b, double c) { return __
 // Warp path for small work items: one warp joins one item on its own, with no
 // block-wide barrier.  The item's queries (at most 32 / D of them per pass) sit
 // in lane registers and are broadcast with shuffles; every lane resolves its
-// own stencil rows through the cell hash (RPL rows per round) and walks their
-// candidates, the warp stepping together through the longest row of the round.
+// own stencil rows through the cell hash (RPL rows per round), and the round's
+// row ranges are laid end to end: in each step the 32 lanes take 32 consecutive
+// candidates of that concatenation (each lane following its own pointer through
+// the ranges), so a round costs ceil(candidates / 32) steps however the
+// candidates spread over its rows.
 // Used once the workload order reaches items with nq * D <= 32 and at most
 // 4096 candidate pairs, when k >= 4 (3^(k-1) >= 27 stencil rows per item):
 // there the block path's barriers and staging cost more than the pairs.
+constexpr uint32_t kWarpRPL = 4;
+
 template <typename T, int D>
 __device__ __forceinline__ void warp_item(const PlainArgs<T>& a, const HjBlock& blk, WarpChunk& wc, uint32_t* wsm,
-                                          unsigned long long& item_cnt) {
+                                          uint32_t* wrng, unsigned long long& item_cnt) {
     constexpr uint32_t G = 32u / D;      // queries per pass
-    constexpr uint32_t RPL = 4;          // stencil rows per lane per round
+    constexpr uint32_t RPL = kWarpRPL;   // stencil rows per lane per round
     const uint32_t lane = lane_id();
     const uint32_t k = a.grid.k;
     const uint32_t nq = blk.q1 - blk.q0;
@@ -141,38 +146,57 @@ __device__ __forceinline__ void warp_item(const PlainArgs<T>& a, const HjBlock& 
                     len[sl] = sp.y - sp.x;
                 }
             }
+            // the round's ranges end to end: range j = sl * 32 + lane starts at candidate
+            // offset pre[j] of the concatenation (pre[32 * RPL] = the round's candidates)
+            uint32_t* rst = wrng;                     // [32 * RPL] range starts (sorted positions)
+            uint32_t* pre = wrng + 32 * RPL;          // [32 * RPL + 1] exclusive prefix of the lengths
+            uint32_t run = 0;
 #pragma unroll
             for (uint32_t sl = 0; sl < RPL; ++sl) {
-                const uint32_t steps = __reduce_max_sync(0xffffffffu, len[sl]);
-                for (uint32_t jj = 0; jj < steps; ++jj) {
-                    const bool valid = jj < len[sl];
-                    const uint32_t p = st[sl] + jj;
-                    T cv[D];
+                uint32_t incl = len[sl];
 #pragma unroll
-                    for (int l = 0; l < D; ++l) cv[l] = valid ? a.pts[(size_t)p * D + l] : T(0);
-                    uint32_t mask = 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= (uint32_t)o) incl += t;
+                }
+                rst[sl * 32 + lane] = st[sl];
+                pre[sl * 32 + lane] = run + incl - len[sl];
+                run += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) pre[32 * RPL] = run;
+            __syncwarp();
+            uint32_t j = 0;   // this lane's current range
+            for (uint32_t base = 0; base < run; base += 32) {
+                const uint32_t idx = base + lane;
+                const bool valid = idx < run;
+                while (j + 1 < 32 * RPL && pre[j + 1] <= idx) ++j;
+                const uint32_t p = valid ? rst[j] + (idx - pre[j]) : 0u;
+                T cv[D];
 #pragma unroll
-                    for (uint32_t qi = 0; qi < G; ++qi) {
-                        T acc = T(0);
+                for (int l = 0; l < D; ++l) cv[l] = valid ? a.pts[(size_t)p * D + l] : T(0);
+                uint32_t mask = 0;
 #pragma unroll
-                        for (int l = 0; l < D; ++l) {
-                            const T q = __shfl_sync(0xffffffffu, qv, qi * D + l);
-                            const T diff = fsub(cv[l], q);   // candidate - query (kernel.cu:351)
-                            acc = ffma(diff, diff, acc);
-                        }
-                        mask |= (uint32_t)(valid && qi < gq && acc <= a.thr) << qi;
+                for (uint32_t qi = 0; qi < G; ++qi) {
+                    T acc = T(0);
+#pragma unroll
+                    for (int l = 0; l < D; ++l) {
+                        const T q = __shfl_sync(0xffffffffu, qv, qi * D + l);
+                        const T diff = fsub(cv[l], q);   // candidate - query (kernel.cu:351)
+                        acc = ffma(diff, diff, acc);
                     }
-                    if (a.count_only) {
-                        item_cnt += __popc(mask);
-                    } else {
-                        cid_w[lane] = valid ? a.perm[p] : 0u;
-                        __syncwarp();
-                        warp_emit_masks(a.sink, wc, mask,
-                                        [&](uint32_t owner, uint32_t b) { return make_uint2(qid_w[b], cid_w[owner]); });
-                        __syncwarp();
-                    }
+                    mask |= (uint32_t)(valid && qi < gq && acc <= a.thr) << qi;
+                }
+                if (a.count_only) {
+                    item_cnt += __popc(mask);
+                } else {
+                    cid_w[lane] = valid ? a.perm[p] : 0u;
+                    __syncwarp();
+                    warp_emit_masks(a.sink, wc, mask,
+                                    [&](uint32_t owner, uint32_t b) { return make_uint2(qid_w[b], cid_w[owner]); });
+                    __syncwarp();
                 }
             }
+            __syncwarp();   // the next round rewrites the ranges
         }
         __syncwarp();
     }
@@ -195,6 +219,7 @@ __global__ void __launch_bounds__(256, 3) k_refine_plain(PlainArgs<T> a) {
     __shared__ uint32_t s_item;
     __shared__ uint32_t wsum_s[17];   // row-group scan: warp totals, their prefixes, the group total
     __shared__ uint32_t warp_sm[8][64];   // warp path: candidate and query ids per warp
+    __shared__ uint32_t warp_rng[8][2 * 32 * kWarpRPL + 1];   // warp path: a round's row ranges per warp
     constexpr bool kWarpPath = D != 0 && D <= 32;
 
     const uint32_t tid = threadIdx.x;
@@ -225,7 +250,7 @@ __global__ void __launch_bounds__(256, 3) k_refine_plain(PlainArgs<T> a) {
                 }
                 while (it_w < a.nblocks) {
                     unsigned long long cnt_w = 0;
-                    warp_item<T, D>(a, a.blocks[it_w], wc, warp_sm[wid], cnt_w);
+                    warp_item<T, D>(a, a.blocks[it_w], wc, warp_sm[wid], warp_rng[wid], cnt_w);
                     if (a.count_only) {
                         for (int o = 16; o > 0; o >>= 1) cnt_w += __shfl_down_sync(0xffffffffu, cnt_w, o);
                         if (lane_id() == 0 && cnt_w) atomicAdd(&a.block_counts[it_w], cnt_w);
