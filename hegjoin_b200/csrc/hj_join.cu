@@ -149,8 +149,8 @@ __global__ void k_gather_items(const HjBlock* __restrict__ in, const uint32_t* _
 struct JoinCtl {
     unsigned long long cursor;        // pair sink cursor of the current batch
     unsigned long long valid;         // pairs left after grouping (sentinels dropped)
-    unsigned long long tc_acc;        // tensor-core filter: pairs accepted outside the band
-    unsigned long long tc_band;       // tensor-core filter: band pairs
+    unsigned long long tc_acc;        // tensor-core filter: pairs accepted outside the band (this batch)
+    unsigned long long tc_band;       // tensor-core filter: band pairs (this batch)
     unsigned long long band_cursor;   // band sink cursor of the current batch
     uint32_t head;                    // work-item queue head of the current launch
     uint32_t overflow;                // a sink ran out of room
@@ -158,7 +158,8 @@ struct JoinCtl {
     uint32_t pad_;
 };
 
-// Start of a batch: both sink cursors, the overflow flag and the queue head.
+// Start of a batch: both sink cursors, the overflow flag, the queue head and the
+// filter's counters (the host adds up those of the batches that did not overflow).
 __global__ void k_batch_reset(JoinCtl* c) {
     if (threadIdx.x == 0) {
         c->cursor = 0;
@@ -166,10 +167,11 @@ __global__ void k_batch_reset(JoinCtl* c) {
         c->valid = 0;
         c->overflow = 0;
         c->head = 0;
+        c->tc_acc = 0;
+        c->tc_band = 0;
     }
 }
 
-// Number of non-sentinel keys in a sorted key array (sentinels sort last).
 // Grouping a batch's pairs by query id: a counting sort.  Keys are query ids
 // below n (sentinel slots are skipped), so one pass counts the pairs per query,
 // an exclusive scan over the n + 1 counters gives every query's first slot, and
@@ -987,6 +989,8 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
             S.n_retries++;
             continue;
         }
+        S.tc_accepts += hc.tc_acc;
+        S.band_pairs += hc.tc_band;
         auto t_g = std::chrono::steady_clock::now();
         const uint64_t slots = std::min<uint64_t>(used, cap);
         uint32_t valid = 0;
@@ -1049,13 +1053,6 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
         S.refine_launches++;
     }
     cudaGetLastError();
-    if (tc) {
-        unsigned long long tcs[2] = {0, 0};
-        HJ_CUDA(cudaMemcpyAsync(tcs, &ctl->tc_acc, sizeof(tcs), cudaMemcpyDeviceToHost, st));
-        HJ_CUDA(cudaStreamSynchronize(st));
-        S.tc_accepts = tcs[0];
-        S.band_pairs = tcs[1];
-    }
     S.total_pairs = total;
     S.n_batches = n_out;
     S.ms_total = ms_since(t_start);
