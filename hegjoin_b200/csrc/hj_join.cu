@@ -738,6 +738,17 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
     S.ms_setup = ms_since(t_start);
     uint32_t stride = std::max<uint32_t>(1, (uint32_t)std::lround(1.0 / opts.sample_rate));
     uint32_t nsamp = nblocks ? (nblocks + stride - 1) / stride : 0;
+    {
+        // a sample of a few persistent-kernel rounds ends with a partly filled round, which
+        // costs as much as a full one: take whole rounds (a multiple of the SM count), at
+        // most the requested rate
+        const uint32_t sms = (uint32_t)num_sms();
+        if (nsamp > sms && nsamp < 8 * sms) {
+            const uint32_t want = (nsamp / sms) * sms;
+            stride = (nblocks + want - 1) / want;
+            nsamp = (nblocks + stride - 1) / stride;
+        }
+    }
     double total_est = 0, cand_total = 0;
     double* pest = nullptr;   // exclusive prefix of the per-item estimates (nblocks + 1)
     double* dsum = nullptr;
