@@ -426,13 +426,19 @@ hj_status index_create_t(const T* d_db, uint32_t n, uint32_t d, uint32_t k, T ep
 // The key word pair is claimed with a 64-bit compare-and-swap on the entry's
 // first 8 bytes; first cell and mask are written after it.
 __global__ void k_hash_insert(const unsigned long long* __restrict__ lid, uint32_t nC, uint4* entries,
-                              unsigned long long mask) {
+                              unsigned long long mask, uint32_t* occ, unsigned long long occ_mask) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nC) return;
     const unsigned long long g = lid[i] >> 2;
     if (i > 0 && (lid[i - 1] >> 2) == g) return;
     uint32_t m = 0;
     for (uint32_t j = i; j < nC && j < i + 4 && (lid[j] >> 2) == g; ++j) m |= 1u << (uint32_t)(lid[j] & 3u);
+    if (occ) {
+        unsigned long long w;
+        uint32_t b;
+        occ_bits(g, occ_mask, &w, &b);
+        atomicOr(occ + w, b);
+    }
     unsigned long long s = mix64(g) & mask;
     for (unsigned long long probe = 0; probe <= mask; ++probe) {   // the table is at most half full
         unsigned long long* kw = reinterpret_cast<unsigned long long*>(&entries[s]);
@@ -446,17 +452,28 @@ __global__ void k_hash_insert(const unsigned long long* __restrict__ lid, uint32
     }
 }
 
+// Smallest table (entries) that gets an occupancy filter: 32 MB of entries.
+constexpr unsigned long long kOccMinCap = 1ull << 21;
+
 // The cell hash of an index whose cell table is built (capacity: the power of
 // two at least twice the number of cells, an upper bound on the groups that
-// needs no count from the device, at least 64).
+// needs no count from the device, at least 64).  From kOccMinCap entries on, an
+// occupancy filter of capacity / 4 words (16 bits per cell, a sixteenth of the
+// table's bytes) goes with it.
 hj_status build_cell_hash(hj_index* ix, cudaStream_t st) {
     unsigned long long cap = 64;
     while (cap < 2ull * ix->nC) cap <<= 1;
     HJ_TRY(dalloc(&ix->hash_entries, (size_t)cap, st));
     HJ_CUDA(cudaMemsetAsync(ix->hash_entries, 0xFF, (size_t)cap * sizeof(uint4), st));
     ix->hash_mask = cap - 1;
+    if (cap >= kOccMinCap) {
+        HJ_TRY(dalloc(&ix->hash_occ, (size_t)(cap / 4), st));
+        HJ_CUDA(cudaMemsetAsync(ix->hash_occ, 0, (size_t)cap, st));
+        ix->occ_mask = cap / 4 - 1;
+    }
     if (ix->nC) {
-        k_hash_insert<<<(ix->nC + 255) / 256, 256, 0, st>>>(ix->cell_lid, ix->nC, ix->hash_entries, ix->hash_mask);
+        k_hash_insert<<<(ix->nC + 255) / 256, 256, 0, st>>>(ix->cell_lid, ix->nC, ix->hash_entries, ix->hash_mask,
+                                                           ix->hash_occ, ix->occ_mask);
         HJ_LAUNCHED();
     }
     return HJ_OK;
@@ -465,6 +482,7 @@ hj_status build_cell_hash(hj_index* ix, cudaStream_t st) {
 void free_index(hj_index* ix, cudaStream_t st) {
     tc_release(ix);
     dfree(ix->hash_entries, st);
+    dfree(ix->hash_occ, st);
     dfree(ix->pts, st);
     dfree(ix->perm, st);
     dfree(ix->cell_lid, st);

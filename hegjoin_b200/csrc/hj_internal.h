@@ -21,9 +21,16 @@ struct HjGrid {
 // power of two at least twice the number of cells (so at most half full of
 // groups); free entries hold the key
 // kEmptyLid (no group can have it: linear ids stay below 2^63).
+// A table too large for L2 gets an occupancy filter beside it: two bits of one
+// 32-bit word per group (16 bits per cell), set at insertion.  A probe of an
+// absent group, the common case on sparse data, then costs one load of a
+// filter small enough to stay in L2 instead of a random DRAM read of the table;
+// about 2% of absent groups pass the filter and read the table as before.
 struct HjCellHash {
     const uint4* entries;
-    unsigned long long mask;   // capacity - 1
+    unsigned long long mask;       // capacity - 1
+    const uint32_t* occ;           // occupancy filter, or null (small tables)
+    unsigned long long occ_mask;   // filter words - 1
 };
 
 // Work item of the refine kernels: queries q0..q1 (sorted positions) of cell
@@ -55,6 +62,8 @@ struct hj_index {
     uint32_t nC = 0;
     uint4* hash_entries = nullptr;   // cell hash (HjCellHash)
     unsigned long long hash_mask = 0;
+    uint32_t* hash_occ = nullptr;    // its occupancy filter (large tables only)
+    unsigned long long occ_mask = 0;
 
     // workload (hj_sort_by_workload)
     bool have_workload = false;
@@ -92,7 +101,18 @@ hj_status build_blocks(const hj_index* ix, uint32_t qb, HjBlock** d_blocks, uint
 constexpr unsigned long long kEmptyLid = ~0ull;
 constexpr uint32_t kNoCell = 0xFFFFFFFFu;
 
-inline HjCellHash cell_hash(const hj_index* ix) { return HjCellHash{ix->hash_entries, ix->hash_mask}; }
+inline HjCellHash cell_hash(const hj_index* ix) {
+    return HjCellHash{ix->hash_entries, ix->hash_mask, ix->hash_occ, ix->occ_mask};
+}
+
+// The filter word of group g and the two bits the group sets in it (a second
+// hash of g, independent of the slot index).
+__host__ __device__ __forceinline__ void occ_bits(unsigned long long g, unsigned long long occ_mask,
+                                                  unsigned long long* word, uint32_t* bits) {
+    const uint64_t z = mix64(g ^ 0xD6E8FEB86659FD93ull);
+    *word = z & occ_mask;
+    *bits = (1u << (uint32_t)((z >> 52) & 31u)) | (1u << (uint32_t)((z >> 58) & 31u));
+}
 
 // Coordinate of the cell with linear id L along dimension lane_id() for the
 // lanes below k: the warp pays one 64-bit division per lane, and the other
@@ -114,6 +134,12 @@ __device__ __forceinline__ uint32_t div_w(uint32_t r, uint32_t w) {
 // no cell.  Probes stop at a free entry; the table is at most half full, so the
 // loop ends after a few probes (and after capacity probes at the very most).
 __device__ __forceinline__ uint2 group_find(const HjCellHash& h, unsigned long long g) {
+    if (h.occ) {
+        unsigned long long w;
+        uint32_t b;
+        occ_bits(g, h.occ_mask, &w, &b);
+        if ((__ldg(h.occ + w) & b) != b) return make_uint2(kNoCell, 0u);
+    }
     unsigned long long i = mix64(g) & h.mask;
     for (unsigned long long probe = 0; probe <= h.mask; ++probe) {
         const uint4 e = h.entries[i];
