@@ -264,16 +264,9 @@ __global__ void k_cell_workload(const unsigned long long* __restrict__ cell_lid,
     }
     unsigned long long cnt = 0;
     if (!empty) {
+        const StencilRows sr = stencil_rows(grid, lo, rows);
         for (uint32_t r = lane_id(); r < rows; r += 32) {
-            uint32_t rem = r;
-            unsigned long long base = 0;
-            for (uint32_t j = 1; j < grid.k; ++j) {
-                const uint32_t qw = div_w(rem, w[j]);
-                uint32_t t = lo[j] + (rem - qw * w[j]);
-                rem = qw;
-                base += (unsigned long long)t * grid.mult[j];
-            }
-            const uint2 sp = cell_span(hash, cell_start, base + lo[0], w[0]);
+            const uint2 sp = cell_span(hash, cell_start, stencil_row_id(grid, sr, lo, w, r), w[0]);
             cnt += sp.y - sp.x;
         }
     }
@@ -452,6 +445,31 @@ __global__ void k_hash_insert(const unsigned long long* __restrict__ lid, uint32
     }
 }
 
+// The grid's row-offset table (HjGrid::row_off), for k <= kRowOffMaxK.
+__global__ void k_row_offsets(HjGrid g, unsigned long long* off) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.full_rows) return;
+    uint32_t rem = r;
+    unsigned long long o = 0;
+    for (uint32_t j = 1; j < g.k; ++j) {
+        o += (unsigned long long)(rem % 3u) * g.mult[j];
+        rem /= 3u;
+    }
+    off[r] = o;
+}
+
+hj_status build_row_offsets(hj_index* ix, cudaStream_t st) {
+    if (ix->grid.k == 0 || ix->grid.k > kRowOffMaxK) return HJ_OK;
+    uint32_t rows = 1;
+    for (uint32_t j = 1; j < ix->grid.k; ++j) rows *= 3;
+    HJ_TRY(dalloc(&ix->row_off, rows, st));
+    ix->grid.full_rows = rows;
+    k_row_offsets<<<(rows + 255) / 256, 256, 0, st>>>(ix->grid, ix->row_off);
+    HJ_LAUNCHED();
+    ix->grid.row_off = ix->row_off;
+    return HJ_OK;
+}
+
 // Smallest table (entries) that gets an occupancy filter: 32 MB of entries.
 constexpr unsigned long long kOccMinCap = 1ull << 21;
 
@@ -483,6 +501,9 @@ void free_index(hj_index* ix, cudaStream_t st) {
     tc_release(ix);
     dfree(ix->hash_entries, st);
     dfree(ix->hash_occ, st);
+    dfree(ix->row_off, st);
+    ix->grid.row_off = nullptr;
+    ix->grid.full_rows = 0;
     dfree(ix->pts, st);
     dfree(ix->perm, st);
     dfree(ix->cell_lid, st);
@@ -609,6 +630,7 @@ hj_status hj_index_create(const void* d_db, uint32_t n, uint32_t d, uint32_t k, 
                       : index_create_t<double>((const double*)d_db, n, d, k, eps, h_min_arr, h_n_cells, st, ix);
     // linear ids are below totalCells <= 2^64 - 1, so none equals the hash's free-slot mark
     if (s == HJ_OK) s = build_cell_hash(ix, st);
+    if (s == HJ_OK) s = build_row_offsets(ix, st);
     if (s != HJ_OK) {
         free_index(ix, st);
         cudaStreamSynchronize(st);

@@ -8,7 +8,14 @@ struct HjGrid {
     uint32_t k;
     uint32_t n_cells[hj::kMaxK];
     unsigned long long mult[hj::kMaxK];   // mixed-radix multipliers, dimension 0 fastest
+    // Row offsets of a full stencil box (width 3 along every dimension j >= 1):
+    // entry r is sum over j >= 1 of digit_j(r) * mult[j], the base-3 digits of r
+    // with dimension 1 fastest; full_rows = 3^(k-1) entries.  Null (and
+    // full_rows 0) for k > kRowOffMaxK.
+    const unsigned long long* row_off;
+    uint32_t full_rows;
 };
+constexpr uint32_t kRowOffMaxK = 7;   // at most 729 offsets
 
 // Open-addressing hash of the non-empty cells, keyed by groups of four
 // consecutive linear ids (g = lid >> 2).  An entry is 16 bytes: the group key
@@ -64,6 +71,7 @@ struct hj_index {
     unsigned long long hash_mask = 0;
     uint32_t* hash_occ = nullptr;    // its occupancy filter (large tables only)
     unsigned long long occ_mask = 0;
+    unsigned long long* row_off = nullptr;   // grid.row_off
 
     // workload (hj_sort_by_workload)
     bool have_workload = false;
@@ -128,6 +136,38 @@ __device__ __forceinline__ uint32_t lane_cell_coord(const HjGrid& g, unsigned lo
 // the stencil is clamped at the grid's edge): no integer division instruction.
 __device__ __forceinline__ uint32_t div_w(uint32_t r, uint32_t w) {
     return w == 3u ? (uint32_t)(((unsigned long long)r * 0xAAAAAAABull) >> 33) : (w == 2u ? r >> 1 : r);
+}
+
+// Stencil rows of a cell's box (per dimension j the cells lo[j] .. lo[j] + w[j] - 1;
+// `rows` is the product of w[1..k-1]).  Row r covers, along dimension j >= 1,
+// coordinate lo[j] + the j-th mixed-radix digit of r (radices w[1], w[2], ...,
+// dimension 1 fastest) and, along dimension 0, the w[0] cells from lo[0].
+// A full box (every w[j] == 3 for j >= 1: the cell is not at the grid's upper
+// edge) reads its rows' offsets from the grid's table; an edge box divides.
+struct StencilRows {
+    bool full;                  // offsets from grid.row_off
+    unsigned long long first;   // linear id of row 0's first cell
+};
+__device__ __forceinline__ StencilRows stencil_rows(const HjGrid& g, const uint32_t* lo, uint32_t rows) {
+    StencilRows s;
+    s.full = g.row_off != nullptr && rows == g.full_rows;
+    s.first = lo[0];
+    for (uint32_t j = 1; j < g.k; ++j) s.first += (unsigned long long)lo[j] * g.mult[j];
+    return s;
+}
+// Linear id of the first cell of row r (equal, modulo 2^64 like all linear-id
+// arithmetic here, in both forms).
+__device__ __forceinline__ unsigned long long stencil_row_id(const HjGrid& g, const StencilRows& s,
+                                                             const uint32_t* lo, const uint32_t* w, uint32_t r) {
+    if (s.full) return s.first + __ldg(g.row_off + r);
+    uint32_t rem = r;
+    unsigned long long id = lo[0];
+    for (uint32_t j = 1; j < g.k; ++j) {
+        const uint32_t qw = div_w(rem, w[j]);
+        id += (unsigned long long)(lo[j] + (rem - qw * w[j])) * g.mult[j];
+        rem = qw;
+    }
+    return id;
 }
 
 // The entry of group g: (first cell, id mask), or a zero mask when the group has

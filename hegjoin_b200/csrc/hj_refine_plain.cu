@@ -118,6 +118,7 @@ __device__ __forceinline__ void warp_item(const PlainArgs<T>& a, const HjBlock& 
         if (j > 0) rows *= w[j];
     }
     if (empty) return;
+    const StencilRows sr = stencil_rows(a.grid, lo, rows);
     uint32_t* cid_w = wsm;        // [32] candidate ids of the current step
     uint32_t* qid_w = wsm + 32;   // [32] original ids of the current pass's queries
     for (uint32_t qg = 0; qg < nq; qg += G) {
@@ -134,14 +135,7 @@ __device__ __forceinline__ void warp_item(const PlainArgs<T>& a, const HjBlock& 
                 st[sl] = 0;
                 len[sl] = 0;
                 if (r < rows) {
-                    uint32_t rem = r;
-                    unsigned long long base = 0;
-                    for (uint32_t j = 1; j < k; ++j) {
-                        const uint32_t qw = div_w(rem, w[j]);
-                        base += (unsigned long long)(lo[j] + (rem - qw * w[j])) * a.grid.mult[j];
-                        rem = qw;
-                    }
-                    const uint2 sp = cell_span(a.hash, a.cell_start, base + lo[0], w[0]);
+                    const uint2 sp = cell_span(a.hash, a.cell_start, stencil_row_id(a.grid, sr, lo, w, r), w[0]);
                     st[sl] = sp.x;
                     len[sl] = sp.y - sp.x;
                 }
@@ -299,15 +293,9 @@ __global__ void __launch_bounds__(256, 3) k_refine_plain(PlainArgs<T> a) {
                     // scan of the 8 warp totals
                     uint32_t len = 0;
                     if (tid < nr) {
-                        uint32_t rem = row0 + tid;
-                        unsigned long long base = 0;
-                        for (uint32_t j = 1; j < k; ++j) {
-                            const uint32_t qw = div_w(rem, w[j]);
-                            uint32_t t = lo[j] + (rem - qw * w[j]);
-                            rem = qw;
-                            base += (unsigned long long)t * a.grid.mult[j];
-                        }
-                        const uint2 sp = cell_span(a.hash, a.cell_start, base + lo[0], w[0]);
+                        const StencilRows sr = stencil_rows(a.grid, lo, rows);   // not kept across the item
+                        const uint2 sp =
+                            cell_span(a.hash, a.cell_start, stencil_row_id(a.grid, sr, lo, w, row0 + tid), w[0]);
                         rs[tid] = sp.x;
                         len = sp.y - sp.x;
                     }

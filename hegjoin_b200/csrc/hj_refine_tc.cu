@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                 if (j > 0) rows *= w[j];
             }
             if (empty) rows = 0;
+            const StencilRows sr = stencil_rows(a.grid, lo, rows);
             uint32_t tiles_mine[kMaxRanges / 32];
             uint32_t my_tiles = 0;
 #pragma unroll
@@ -310,15 +311,7 @@ __global__ void __launch_bounds__(32 * (1 + kAcc) + 128 * EPI, 1)
                 uint32_t r = lane * (kMaxRanges / 32) + s;
                 uint32_t len = 0, st = 0;
                 if (r < rows) {
-                    uint32_t rem = r;
-                    unsigned long long bse = 0;
-                    for (uint32_t j = 1; j < k; ++j) {
-                        const uint32_t qw = div_w(rem, w[j]);
-                        uint32_t t = lo[j] + (rem - qw * w[j]);
-                        rem = qw;
-                        bse += (unsigned long long)t * a.grid.mult[j];
-                    }
-                    const uint2 sp = cell_span(a.hash, a.cell_start, bse + lo[0], w[0]);
+                    const uint2 sp = cell_span(a.hash, a.cell_start, stencil_row_id(a.grid, sr, lo, w, r), w[0]);
                     st = sp.x;
                     len = sp.y - sp.x;
                     S.rs[r] = st;
