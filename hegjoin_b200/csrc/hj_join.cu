@@ -286,26 +286,17 @@ __global__ void __launch_bounds__(256) k_group_scatter(const uint32_t* __restric
     }
 }
 
-__device__ __forceinline__ unsigned long long lower_bound_u32(const uint32_t* a, unsigned long long n, uint32_t v) {
-    unsigned long long lo = 0, hi = n;
-    while (lo < hi) {
-        unsigned long long mid = (lo + hi) >> 1;
-        if (a[mid] < v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
-// constructNeighborTableKeyValueWithPtrs (GPU.cu:1731-1776) on the device: one
-// entry per run of equal keys, written by the run's last element.
-__global__ void k_table(const uint32_t* __restrict__ keys, unsigned long long n, uint32_t batch,
-                        hj_nt_entry* __restrict__ table) {
-    unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint32_t key = keys[i];
-    if (i + 1 == n || keys[i + 1] != key) {
-        unsigned long long lo = lower_bound_u32(keys, i + 1, key);
-        table[key] = hj_nt_entry{batch, (uint32_t)(i + 1 - lo), lo};
-    }
+// constructNeighborTableKeyValueWithPtrs (GPU.cu:1731-1776) on the device, from
+// the grouping's cursors: after the scatter, run_end[q] is one past query q's last
+// pair in the batch's grouped arrays and its run starts at run_end[q - 1] (0 for
+// q = 0), so every query with pairs gets its entry without a pass over the pairs.
+__global__ void k_table_runs(const uint32_t* __restrict__ run_end, uint32_t n, uint32_t batch,
+                             hj_nt_entry* __restrict__ table) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const uint32_t start = q ? run_end[q - 1] : 0u;
+    const uint32_t end = run_end[q];
+    if (end > start) table[q] = hj_nt_entry{batch, end - start, start};
 }
 
 __global__ void k_table_counts(const hj_nt_entry* __restrict__ t, uint32_t n, uint32_t* __restrict__ cnt) {
@@ -567,9 +558,12 @@ struct BatchHandler {
     virtual ~BatchHandler() = default;
     // `count` pairs of batch `batch`: query ids (ascending) in keys, neighbour ids
     // grouped by query in vals.  Both live in the join's reusable buffers and stay
-    // valid in the order of `st` until the next batch's refine is enqueued.
+    // valid in the order of `st` until the next batch's refine is enqueued.  With
+    // pairs, run_end (n entries, in the order of `st` until the next batch's grouping)
+    // holds one past each query's last pair: query q's run is
+    // [run_end[q - 1] (0 for q = 0), run_end[q]).
     virtual hj_status on_batch(uint32_t batch, const uint32_t* keys, const uint32_t* vals, uint64_t count,
-                               cudaStream_t st) = 0;
+                               const uint32_t* run_end, cudaStream_t st) = 0;
     // Whether the handler can use two alternating sets of grouped arrays, and the event
     // (if any) after which the last batch's set may be reused.
     virtual bool can_overlap() const { return false; }
@@ -1046,7 +1040,7 @@ hj_status join_impl(hj_index* ix, const hj_join_opts* opts_in, cudaStream_t st, 
                 HJ_CUDA(cudaStreamWaitEvent(st, release[set], 0));
                 release[set] = nullptr;
             }
-            HJ_TRY(handler.on_batch(n_out, grp_keys[set], grp_vals[set], valid, st));
+            HJ_TRY(handler.on_batch(n_out, grp_keys[set], grp_vals[set], valid, valid ? qoff : nullptr, st));
             release[set] = handler.take_release();
         }
         ++n_out;
@@ -1079,7 +1073,7 @@ struct RetainHandler : BatchHandler {
     bool keep_keys;
     RetainHandler(hj_result* r, bool kk) : res(r), keep_keys(kk) {}
     hj_status on_batch(uint32_t bi, const uint32_t* keys, const uint32_t* vals, uint64_t count,
-                       cudaStream_t st) override {
+                       const uint32_t* run_end, cudaStream_t st) override {
         uint32_t* bv = nullptr;
         HJ_TRY(dalloc(&bv, count, st));
         res->vals.push_back(bv);
@@ -1092,7 +1086,7 @@ struct RetainHandler : BatchHandler {
             if (count) HJ_CUDA(cudaMemcpyAsync(bk, keys, count * 4, cudaMemcpyDeviceToDevice, st));
         }
         if (count) {
-            k_table<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(keys, count, bi, res->table);
+            k_table_runs<<<(res->n + 255) / 256, 256, 0, st>>>(run_end, res->n, bi, res->table);
             HJ_LAUNCHED();
         }
         res->total += count;
@@ -1112,7 +1106,7 @@ struct StreamHandler : BatchHandler {
         : sink(s), user(u), cnt(c), sum(reinterpret_cast<unsigned long long*>(sm)),
           xr(reinterpret_cast<unsigned long long*>(x)) {}
     hj_status on_batch(uint32_t bi, const uint32_t* keys, const uint32_t* vals, uint64_t count,
-                       cudaStream_t st) override {
+                       const uint32_t* /*run_end*/, cudaStream_t st) override {
         if (count && cnt) {
             const uint64_t per_block = 8ull * kDigestSpan;   // 8 warps, each a walk of 512 pairs
             const unsigned g = (unsigned)std::min<uint64_t>((count + per_block - 1) / per_block, (uint64_t)num_sms() * 16);
